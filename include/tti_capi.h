@@ -1,0 +1,274 @@
+/*
+ * tti_capi.h -- C ABI of the B200 TTI/VTI pseudo-acoustic RTM library
+ * (libtti_b200.so).
+ *
+ * Drop-in boundary for the hot path of MiniAppsForHPE's simulator2 /
+ * kernels/ (paths below are relative to the reference's simulatorsForNvidia/
+ * directory).  Two levels, as in the reference:
+ *
+ *   1. Per-kernel launchers with the reference launchers' argument lists and
+ *      meaning: raw device pointers to FP32 volumes in the reference layout
+ *      (x fastest, radius-4 halo on every axis, ldimx padded to 32 floats),
+ *      inclusive interior index ranges, leading dimensions and a stream.
+ *   2. A simulator object covering the simulator2SetUp call surface: grid
+ *      and model setup, source, receivers, forward and adjoint time loops,
+ *      device-resident snapshot save/restore, imaging condition, image
+ *      readback.
+ *
+ * Error convention: where the reference aborts (CUDA_TRY / EMSL_VERIFY,
+ * utils/cuda_utils.h:20-60, utils/emsl_error.h:21) every entry point here
+ * returns a status code instead.  Nothing in the library aborts.
+ *
+ * Streams are passed as void* (a cudaStream_t); NULL is the legacy default
+ * stream, which is what the reference simulator uses (kernel_base.h:32-40).
+ * Only order 8 is supported, the order the reference simulator runs
+ * (simulator2SetUp.h:103); other orders return TTI_EINVAL.
+ */
+#ifndef TTI_CAPI_H
+#define TTI_CAPI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    TTI_OK = 0,
+    TTI_EINVAL = 1,   /* bad argument or unsupported configuration */
+    TTI_ENOMEM = 2,   /* device or pinned-host allocation failed */
+    TTI_ELAUNCH = 3,  /* kernel launch or CUDA runtime error */
+    TTI_ETIMEOUT = 4, /* a bounded wait gave up */
+    TTI_ESTATE = 5    /* call out of order (e.g. read before any write) */
+};
+
+typedef void* tti_stream_t;
+
+/* Human-readable name of a status code (static string). */
+const char* tti_status_string(int status);
+/* Library version, e.g. "0.1.0" (static string). */
+const char* tti_version(void);
+
+/* ------------------------------------------------------------------------
+ * 1. Per-kernel launchers.  Device pointers; the caller owns every volume
+ *    (as cart_volume_regular_gpu owns them in the reference).
+ * ---------------------------------------------------------------------- */
+
+/* Six staggered first derivatives (shift -1/2) times buoyancy Model11.
+ * Replaces kernel3_gpu_kernels::launch_fwd_kernel2_drv
+ * (kernels/kernel_type2_fwd_drv.h:7-11). */
+int tti_launch_fwd_kernel2_drv(const float* field1, const float* field2, const float* Model11, float* dfield1dx,
+                               float* dfield1dy, float* dfield1dz, float* dfield2dx, float* dfield2dy,
+                               float* dfield2dz, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+                               float invdx, float invdy, float invdz, int ldimx, int ldimy, int order,
+                               tti_stream_t stream);
+
+/* Forward TTI update field3/field4 += dt*rhs.  Replaces
+ * launch_update_rho_fwd_main_loop_2_1 (kernels/kernel_type2_fwd.h:6-14).
+ * The PML arguments must be NULL and pml_x/y/z false: the reference never
+ * instantiates its PML path (kernel_type2_fwd.cu:641).  sponge_active is
+ * accepted and ignored, as in the reference launcher (kernel_type2_fwd.cu:641
+ * instantiates sponge_active=false). */
+int tti_launch_update_rho_fwd_main_loop_2_1(
+    float* field3, float* field4, const float* field1_dx, const float* field2_dx, const float* field1_dy,
+    const float* field2_dy, const float* field1_dz, const float* field2_dz, const float* field1, const float* field2,
+    const float* irho, const float* model1, const float* model2, const float* model3, const float* model4,
+    const float* rx, const float* ry, const float* rz, float* pml_field1_xx, float* pml_field2_xx,
+    float* pml_field1_yy, float* pml_field2_yy, float* pml_field1_zz, float* pml_field2_zz, const float* pml_ab_x,
+    const float* pml_ab_y, const float* pml_ab_z, const float* sponge_ab_xx, const float* sponge_ab_yy,
+    const float* sponge_ab_zz, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend, int ldimx,
+    int ldimy, float dt, double dx, double dy, double dz, int sponge_active, int order, int pml_x, int pml_y,
+    int pml_z, tti_stream_t stream);
+
+/* Adjoint derivatives and mixed-derivative rhs.  Replaces
+ * adj_kernel3_derivatives::launch_adj_kernel2_drv
+ * (kernels/kernel_type2_grad_snap.h:7-12).  Model volumes must be finite
+ * and Model11 non-zero in the x/y/z halo (the temporaries are formed there). */
+int tti_launch_adj_kernel2_drv(float* dfield1dx, float* dfield2dx, float* dfield1dy, float* dfield2dy,
+                               float* dfield1dz, float* dfield2dz, float* field3_rhs, float* field4_rhs,
+                               const float* field1, const float* field2, const float* Model11, const float* model1,
+                               const float* model2, const float* model3, const float* model4, const float* model5,
+                               const float* model6, const float* model7, int ixbeg, int ixend, int iybeg,
+                               int iyend, int izbeg, int izend, float invdxx, float invdyy, float invdzz,
+                               float invdxy, float invdyz, float invdzx, int ldimx, int ldimy, int order, float dt,
+                               float invdx, float invdy, float invdz, tti_stream_t stream);
+
+/* Adjoint update.  Replaces kernel3_gpu_kernels::launch_update_adj_kernel_main_3
+ * (kernels/kernel_type2_adj.h:8-14).  ab_* are float2 (A,B) sponge arrays
+ * indexed by the global axis index; pml flags must be false. */
+int tti_launch_update_adj_kernel_main_3(float* field3, float* field4, const float* field1_dx,
+                                        const float* field2_dx, const float* field1_dy, const float* field2_dy,
+                                        const float* field1_dz, const float* field2_dz, const float* field3_rhs,
+                                        const float* field4_rhs, const float* ab_xx, const float* ab_yy,
+                                        const float* ab_zz, int ixbeg, int ixend, int iybeg, int iyend, int izbeg,
+                                        int izend, int ldimx, int ldimy, float dt, double dx, double dy, double dz,
+                                        int pmlx, int pmly, int pmlz, int order, int sponge_active,
+                                        tti_stream_t stream);
+
+/* Density gradient grad -= irho*sum(adj*D+fwd + D-adj*fwd).  Replaces
+ * launch_update_rho_gradient_rho (kernels/kernel_type2_grad.h:22-32).
+ * grad is not offset (element 0 is the first interior point) and has its
+ * own leading dimensions, as in the reference. */
+int tti_launch_update_rho_gradient_rho(float* grad, const float* fwd_field1_dx, const float* fwd_field2_dx,
+                                       const float* fwd_field1_dy, const float* fwd_field2_dy,
+                                       const float* fwd_field1_dz, const float* fwd_field2_dz, const float* field1,
+                                       const float* field2, const float* irho, const float* model1,
+                                       const float* model2, const float* model3, const float* model4,
+                                       const float* rx, const float* ry, const float* rz, int ixbeg, int ixend,
+                                       int iybeg, int iyend, int izbeg, int izend, int ldimx, int ldimy,
+                                       int grad_ldimx, int grad_ldimy, double dx, double dy, double dz, int order,
+                                       int simple_gradient, tti_stream_t stream);
+
+/* Free-surface mirror of the six derivative volumes over whole XY planes
+ * iz <= izbeg.  Replaces the kernel3_gpu_kernels::kernel_loop4_derivatives
+ * launch of kernel_type2::kernel_loop4_derivative_impl
+ * (kernels/kernel_type2_small.h:8-9, kernels/kernel_type2.cu:278-293). */
+int tti_launch_kernel_loop4_derivatives(float* dfield1dx, float* dfield1dy, float* dfield1dz, float* dfield2dx,
+                                        float* dfield2dy, float* dfield2dz, int xtot, int ytot, int izbeg,
+                                        tti_stream_t stream);
+
+/* Imaging condition grad_Vp += adj3*snap3 + adj4*snap4 over the interior.
+ * snap/grad have no halo and leading dimensions (snx, sny); adj fields are
+ * halo'd with (ldimx, ldimy).  Replaces the update_Vp_gradient launch of
+ * kernel_type2::update_grad_loop_1_impl (kernels/kernel_type2_small.h:11-14,
+ * kernels/kernel_type2.cu:305-330). */
+int tti_launch_update_Vp_gradient(const float* snap_field3, const float* snap_field4, float* grad_Vp,
+                                  const float* adj_field3, const float* adj_field4, int ixbeg, int ixend, int iybeg,
+                                  int iyend, int izbeg, int izend, int snx, int sny, int ldimx, int ldimy,
+                                  tti_stream_t stream);
+
+/* grad_Vp *= -2*dt_xcorr/sqrt(model3).  kernels/kernel_type2_small.h:16-18. */
+int tti_launch_finalize_Vp_gradient(const float* model3, float* grad_Vp, int ixbeg, int ixend, int iybeg,
+                                    int iyend, int izbeg, int izend, int snx, int sny, int ldimx, int ldimy,
+                                    float dt_xcorr, tti_stream_t stream);
+
+/* p = A*p + B*dt*pdot over the interior; ab_* float2 (A,B) per global index.
+ * Replaces kernel_base::kernel_loop2_inner (kernels/kernel_base.cu:82-140). */
+int tti_launch_kernel_loop2(float* field1, float* field2, const float* field3, const float* field4, int ldimx,
+                            int ldimy, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+                            const float* ab_x, const float* ab_y, const float* ab_z, float dt, tti_stream_t stream);
+
+/* Free surface on p,q: zero at izbeg, odd mirror above, whole XY planes.
+ * Replaces kernel_base::kernel_loop4_inner (kernels/kernel_base.cu:142-187). */
+int tti_launch_kernel_loop4(float* field1, float* field2, int ldimx, int ldimy, int izbeg, tti_stream_t stream);
+
+/* Model parameters from per-cell (vp, eps, delta, vs, theta, phi) over n
+ * cells (any layout, element-wise).  simulator2SetUp.cu:10-29 restated per
+ * cell (the reference takes scalars). */
+int tti_launch_init_cijs(const float* vp, const float* eps, const float* delta, const float* vs,
+                         const float* theta, const float* phi, float* model1, float* model2, float* model3,
+                         float* model4, float* model5, float* model6, float* model7, int64_t n,
+                         tti_stream_t stream);
+
+/* Pressure P = -(2p+q)/3 over n cells.  simulator2SetUp.cu:31-42,842-857. */
+int tti_launch_compute_pressure(float* pressure, const float* field1, const float* field2, int64_t n,
+                                tti_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * 2. Simulator object (simulator2SetUp call surface,
+ *    simulator2/simulator2SetUp.h:25-35, execute at simulator2SetUp.cu:517-814).
+ * ---------------------------------------------------------------------- */
+
+typedef struct tti_sim tti_sim;
+
+typedef struct {
+    int nx, ny, nz;       /* interior grid (the reference's npoints+2*npml per axis) */
+    double dx, dy, dz;    /* spacing (metres) */
+    float dt;             /* time step (seconds) */
+    int nt;               /* time steps (niter) */
+    int xcorr_step;       /* snapshot / imaging cadence */
+    int sponge_width;     /* absorbing cells on each side except a free-surface top; 0 = none */
+    int free_surface;     /* 1: free surface at the top interior plane (reference behaviour) */
+    int fused;            /* 1: fused step kernels; 0: the reference's kernel sequence */
+    int save_snapshots;   /* 1: keep the forward snapshots on the device for the adjoint */
+} tti_sim_config;
+
+int tti_sim_create(const tti_sim_config* cfg, tti_sim** out);
+int tti_sim_destroy(tti_sim* sim);
+
+/* Model from host arrays over the interior (nx*ny*nz, x fastest): vp, eps,
+ * delta, vs (m/s), theta, phi (radians), rho.  Halos are filled by edge
+ * extension.  Any pointer may be NULL for its default (eps=delta=vs=theta=phi=0,
+ * rho=1). */
+int tti_sim_set_model(tti_sim* sim, const float* vp, const float* eps, const float* delta, const float* vs,
+                      const float* theta, const float* phi, const float* rho);
+
+/* Point source at interior cell (ix,iy,iz): pdot,qdot += w[n]*dt each step. */
+int tti_sim_set_source(tti_sim* sim, int ix, int iy, int iz, const float* wavelet_host, int nt);
+
+/* Receivers at interior cells (3*nrec ints: ix,iy,iz per receiver, distinct).
+ * They record P = -(2p+q)/3 every step. */
+int tti_sim_set_receivers(tti_sim* sim, int nrec, const int* ixyz_host);
+
+/* Forward time loop (nt steps).  traces: nt*nrec floats, host memory if
+ * traces_on_device is 0 else device memory; may be NULL. */
+int tti_sim_forward(tti_sim* sim, float* traces, int traces_on_device);
+
+/* Adjoint time loop seeded with residual traces (nt*nrec, same placement
+ * rule), imaging condition at every snapshot step (Vp and rho gradients). */
+int tti_sim_adjoint(tti_sim* sim, const float* residual, int residual_on_device);
+
+/* Adjoint loop whose residual is formed on the device from the synthetic
+ * traces of the last forward run minus these observed traces (nt*nrec). */
+int tti_sim_adjoint_observed(tti_sim* sim, const float* observed, int observed_on_device);
+
+/* Image readback: Vp gradient (finalised, -2*dt*xcorr/vp) and rho gradient,
+ * nx*ny*nz each, host or device memory. */
+int tti_sim_get_image(tti_sim* sim, float* grad_vp, float* grad_rho, int on_device);
+
+/* Gradient of the receiver misfit of the last adjoint run with respect to
+ * each source wavelet sample: dt*(adjoint p + q) at the source cell, nt
+ * floats into host memory.  Together with tti_sim_forward this gives the
+ * forward/adjoint pair a dot-product test can check. */
+int tti_sim_source_gradient(tti_sim* sim, float* host_out);
+
+/* Device pointer of an internal volume for inspection: which = 0..3 for
+ * field1..field4 (p, q, pdot, qdot), 4..11 for irho, model1..model4, rx, ry, rz. */
+int tti_sim_volume(tti_sim* sim, int which, float** dev_ptr);
+
+/* Copy one internal volume (same numbering as tti_sim_volume) to host
+ * memory: ldimx*ldimy*ldimz floats. */
+int tti_sim_read_volume(tti_sim* sim, int which, float* host_dst);
+
+/* Layout of the simulator's volumes: ldimx, ldimy, ldimz. */
+int tti_sim_layout(tti_sim* sim, int* ldimx, int* ldimy, int* ldimz);
+
+/* Per-launch timing of the step kernels with CUDA events on the simulator's
+ * stream (enable resets the totals).  tti_sim_kernel_times fills ms[3] and
+ * launches[3] for: 0 forward step kernel, 1 adjoint step kernel, 2 imaging. */
+int tti_sim_set_profiling(tti_sim* sim, int enable);
+int tti_sim_kernel_times(tti_sim* sim, double* ms, int64_t* launches);
+
+/* Kernel launches issued by the last forward/adjoint call. */
+int64_t tti_sim_launch_count(tti_sim* sim);
+
+/* Stream the simulator runs on (a cudaStream_t). */
+tti_stream_t tti_sim_stream(tti_sim* sim);
+
+/* ------------------------------------------------------------------------
+ * 3. Device-resident snapshot store with the rtm_snap call sequence
+ *    (snap_helpers/rtm_snap.h:19-41): LIFO, written on the forward pass,
+ *    read back in reverse on the adjoint pass.  Each snapshot holds nvol
+ *    volumes of the given element counts.
+ * ---------------------------------------------------------------------- */
+typedef struct tti_snap_store tti_snap_store;
+
+int tti_snap_create(int nvol, const int64_t* nelem, int capacity, tti_snap_store** out);
+int tti_snap_destroy(tti_snap_store* s);
+/* Waits for the previous write to have drained (rtm_snap lock_for_write). */
+int tti_snap_lock_for_write(tti_snap_store* s);
+/* Copies the nvol device volumes into the next slot, ordered after work
+ * already queued on stream (rtm_snap start_write). */
+int tti_snap_start_write(tti_snap_store* s, float* const* vols, tti_stream_t stream);
+/* Starts copying the most recent unread slot into the nvol device volumes
+ * (rtm_snap start_read); TTI_ESTATE when the store is empty. */
+int tti_snap_start_read(tti_snap_store* s, float* const* vols, tti_stream_t stream);
+/* Orders stream after the pending read (rtm_snap finish_read). */
+int tti_snap_finish_read(tti_snap_store* s, tti_stream_t stream);
+int tti_snap_count(tti_snap_store* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TTI_CAPI_H */

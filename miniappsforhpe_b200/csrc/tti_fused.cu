@@ -1,0 +1,1048 @@
+// Fused time-step kernels for the TTI/VTI pseudo-acoustic RTM on B200.
+//
+// One kernel per forward step and one per adjoint step replace the
+// reference's per-step kernel sequences
+//   forward  (simulator2SetUp.cu:530-651): loop2, loop4, fwd_drv,
+//            loop4_derivatives, fwd_main_loop_2
+//   adjoint  (simulator2SetUp.cu:654-720): adj_drv, loop4_derivatives,
+//            update_adj_kernel_main_3, loop2, loop4
+// so that each step streams every volume through HBM once: p,q are read
+// from one buffer and the next p,q are written to a second one; pdot,qdot
+// are updated in place; the six buoyancy-scaled derivative volumes and the
+// two mixed-derivative volumes of the reference never touch HBM.
+//
+// Structure (2.5D blocking): a CTA owns a 32x16 column tile and marches
+// through a chunk of z.  Halo'd XY planes are staged into shared memory by
+// TMA (cp.async.bulk.tensor, zero fill outside the volume) behind a
+// multi-stage mbarrier pipeline; the z-direction stencils run in per-thread
+// register queues.  The D-z stage of the staggered pair is scattered plane by
+// plane as in the reference kernels; the D+z stage keeps the raw buoyancy-
+// scaled z-derivatives of the last eight planes so the reference's tap order
+// is preserved and the free-surface mirror can be resolved at output time.
+// Output for plane z happens when plane z+7 arrives.
+//
+// Every mbarrier wait is bounded (clock-based); a wait that gives up sets the
+// error word the host reads back, and the kernel stops waiting.
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "tti_common.cuh"
+#include "tti_internal.cuh"
+
+namespace tti {
+namespace {
+
+constexpr int TX = 32, TY = 16, NT = TX * TY;
+constexpr int PW = TX + 16, PH = TY + 16;  // p/q tile with a halo of 8
+constexpr int IW = TX + 8, IH = TY + 8;    // tile with a halo of 4
+constexpr int LAG = 7;                     // output plane = arrival plane - 7
+
+// ---------------------------------------------------------------------------
+// TMA / mbarrier primitives (PTX ISA 8.x, sm_90+).
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(saddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: about a second of SM clocks, then report and give up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, bool& dead)
+{
+    if (dead) return false;
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > (2LL << 30)) {
+            atomicExch(err, 1);
+            dead = true;
+            return false;
+        }
+    }
+    return true;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(saddr(bar))
+        : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Free-surface resolution of the buoyancy-scaled z-derivative queue.
+// q[j] holds the derivative at position z-3+j.  The z-marching pipeline
+// already zeroes positions outside the interior (the reference's derivative
+// volumes are never written in the halo).  With a free surface, positions
+// <= izbeg instead take the value at 2*izbeg+1-pos (kernel_type2_small.cu:
+// 34-39), which is in the queue itself for the four outputs nearest the
+// surface: j' = 7 - 2*(z-izbeg) - j.
+__device__ __forceinline__ void resolve_dz(float (&q)[8], int dtop)
+{
+    switch (dtop) {
+    case 0:
+        q[0] = q[7];
+        q[1] = q[6];
+        q[2] = q[5];
+        q[3] = q[4];
+        break;
+    case 1:
+        q[0] = q[5];
+        q[1] = q[4];
+        q[2] = q[3];
+        break;
+    case 2:
+        q[0] = q[3];
+        q[1] = q[2];
+        break;
+    case 3: q[0] = q[1]; break;
+    default: break;
+    }
+}
+
+// D- z-stage coefficient for a scatter from arrival plane L into queue slot j
+// (position L-3+j): ir = 3-j  ->  +c1(ir+1) for ir>=0, -c1(-ir) for ir<0.
+__device__ __forceinline__ float dminus_coef(int j) { return (j <= 3) ? c1(4 - j) : -c1(j - 3); }
+
+struct FwdParams {
+    float* pout;
+    float* qout;
+    float* f3;
+    float* f4;
+    const float *irho, *m1, *m2, *m3, *m4, *rx, *ry, *rz;
+    const float2 *abx, *aby, *abz;
+    float* snap;
+    int64_t src_index;
+    float src_term;
+    Layout L;
+    int bz;  // z planes per chunk
+    int fs;
+    float dt, invdx, invdy, invdz, invdxdy, invdydz, invdzdx;
+    int* err;
+};
+
+constexpr int FWD_NS = 11;  // ring: planes L-8 .. L+2
+constexpr int FWD_PF = 2;   // prefetch distance
+constexpr size_t FWD_SLOT_P = (size_t)2 * PH * PW * sizeof(float);  // p and q tiles
+constexpr size_t FWD_SLOT_I = (size_t)IH * IW * sizeof(float);      // irho tile
+constexpr size_t FWD_DX = (size_t)2 * TY * IW * sizeof(float);
+constexpr size_t FWD_DY = (size_t)2 * IH * TX * sizeof(float);
+constexpr size_t FWD_SMEM = FWD_NS * (FWD_SLOT_P + FWD_SLOT_I) + FWD_DX + FWD_DY + FWD_NS * sizeof(uint64_t);
+
+template <bool TTI>
+__global__ void __launch_bounds__(NT, 1)
+    k_fused_forward(const __grid_constant__ CUtensorMap tm_p, const __grid_constant__ CUtensorMap tm_q,
+                    const __grid_constant__ CUtensorMap tm_i, const FwdParams a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* ring = reinterpret_cast<float*>(smem);                                  // [NS][2][PH][PW]
+    float* iring = reinterpret_cast<float*>(smem + FWD_NS * FWD_SLOT_P);           // [NS][IH][IW]
+    float* dxs = reinterpret_cast<float*>(smem + FWD_NS * (FWD_SLOT_P + FWD_SLOT_I));  // [2][TY][IW]
+    float* dys = reinterpret_cast<float*>(smem + FWD_NS * (FWD_SLOT_P + FWD_SLOT_I) + FWD_DX);  // [2][IH][TX]
+    uint64_t* bars =
+        reinterpret_cast<uint64_t*>(smem + FWD_NS * (FWD_SLOT_P + FWD_SLOT_I) + FWD_DX + FWD_DY);
+
+    const Layout& L = a.L;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int x0 = L.ixbeg + blockIdx.x * TX, y0 = L.iybeg + blockIdx.y * TY;
+    const int zs = L.izbeg + blockIdx.z * a.bz;
+    const int ze = min(zs + a.bz - 1, L.izend);
+    const int ntot = ze - zs + 1 + 2 * LAG;  // arrival planes zs-7 .. ze+7
+    const int x = x0 + tx, y = y0 + ty;
+    const bool owner = (x <= L.ixend) && (y <= L.iyend);
+    bool dead = false;
+
+    if (tid == 0) {
+        for (int s = 0; s < FWD_NS; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int t) {
+        const int s = t % FWD_NS, z = zs - LAG + t;
+        float* dst = ring + (size_t)s * 2 * PH * PW;
+        mbar_expect_tx(&bars[s], (uint32_t)(FWD_SLOT_P + FWD_SLOT_I));
+        tma_load_3d(dst, &tm_p, x0 - 8, y0 - 8, z, &bars[s]);
+        tma_load_3d(dst + PH * PW, &tm_q, x0 - 8, y0 - 8, z, &bars[s]);
+        tma_load_3d(iring + (size_t)s * IH * IW, &tm_i, x0 - 4, y0 - 4, z, &bars[s]);
+    };
+    if (tid == 0)
+        for (int t = 0; t < FWD_PF && t < ntot; ++t) issue(t);
+
+    float dzq1[8], dzq2[8];  // D- partial sums, positions L-3 .. L+4
+    float dZ1[8], dZ2[8];    // buoyancy-scaled z derivatives, positions L-10 .. L-3
+    float mq[3][4];          // zx1, zx2, yz1, yz2 for outputs L-7, L-6, L-5
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dzq1[j] = dzq2[j] = dZ1[j] = dZ2[j] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) mq[j][c] = 0.0f;
+
+    const int vc = (tx + 8), vr = (ty + 8);  // this column inside a p/q tile
+
+    for (int t = 0; t < ntot; ++t) {
+        __syncthreads();  // every thread is done with iteration t-1
+        if (tid == 0 && t + FWD_PF < ntot) {
+            fence_proxy_async();
+            issue(t + FWD_PF);
+        }
+        const int s = t % FWD_NS;
+        mbar_wait(&bars[s], (uint32_t)((t / FWD_NS) & 1), a.err, dead);
+        const int Lz = zs - LAG + t;
+        const float* P1 = ring + (size_t)s * 2 * PH * PW;
+        const float* P2 = P1 + PH * PW;
+
+        // (a) D- z stage: scatter plane L into positions L-3 .. L+4.
+        {
+            const float v1 = P1[vr * PW + vc], v2 = P2[vr * PW + vc];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float c = dminus_coef(j);
+                dzq1[j] = dzq1[j] + c * v1;
+                dzq2[j] = dzq2[j] + c * v2;
+            }
+        }
+        // completed position L-3: scale by 1/dz and the buoyancy there
+        {
+            const int zp = Lz - 3;
+            const bool valid = (zp >= L.izbeg + (a.fs ? 1 : 0)) && zp <= L.izend;
+            const float* I3 = iring + (size_t)((t + FWD_NS - 3) % FWD_NS) * IH * IW;
+            const float ir3 = I3[(ty + 4) * IW + tx + 4];
+            const float n1 = valid ? (dzq1[0] * a.invdz) * ir3 : 0.0f;
+            const float n2 = valid ? (dzq2[0] * a.invdz) * ir3 : 0.0f;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) {
+                dZ1[j] = dZ1[j + 1];
+                dZ2[j] = dZ2[j + 1];
+                dzq1[j] = dzq1[j + 1];
+                dzq2[j] = dzq2[j + 1];
+            }
+            dZ1[7] = n1;
+            dZ2[7] = n2;
+            dzq1[7] = 0.0f;
+            dzq2[7] = 0.0f;
+        }
+        // (b) mixed zx/yz for output L-4 from planes L-8 .. L (ring), TTI only.
+        float mz[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if constexpr (TTI) {
+#pragma unroll
+            for (int m = -4; m <= 4; ++m) {
+                if (m == 0) continue;
+                const float c = c2(m < 0 ? -m : m);
+                const float* Q1 = ring + (size_t)((t + FWD_NS - 4 + m) % FWD_NS) * 2 * PH * PW;
+                const float* Q2 = Q1 + PH * PW;
+                mz[0] += c * (Q1[vr * PW + vc + m] - Q1[vr * PW + vc - m]);
+                mz[1] += c * (Q2[vr * PW + vc + m] - Q2[vr * PW + vc - m]);
+                mz[2] += c * (Q1[(vr + m) * PW + vc] - Q1[(vr - m) * PW + vc]);
+                mz[3] += c * (Q2[(vr + m) * PW + vc] - Q2[(vr - m) * PW + vc]);
+            }
+            mz[0] *= a.invdzdx;
+            mz[1] *= a.invdzdx;
+            mz[2] *= a.invdydz;
+            mz[3] *= a.invdydz;
+        }
+
+        // (c) output plane L-7
+        const int z = Lz - LAG;
+        if (z >= zs) {  // block-uniform
+            const int s7 = (t + FWD_NS - LAG) % FWD_NS;
+            const float* O1 = ring + (size_t)s7 * 2 * PH * PW;
+            const float* I7 = iring + (size_t)s7 * IH * IW;
+            // issue the point-wise loads of this cell early
+            const int64_t gi = L.idx(x, y, z);
+            float a1 = 0, a2 = 0, a3 = 0, a4 = 0, vrx = 0, vry = 0, vrz = 1, o3 = 0, o4 = 0;
+            float2 sx = make_float2(1, 1), sy = sx, sz = sx;
+            if (owner) {
+                a1 = __ldg(a.m1 + gi);
+                a2 = __ldg(a.m2 + gi);
+                a3 = __ldg(a.m3 + gi);
+                a4 = __ldg(a.m4 + gi);
+                if constexpr (TTI) {
+                    vrx = __ldg(a.rx + gi);
+                    vry = __ldg(a.ry + gi);
+                    vrz = __ldg(a.rz + gi);
+                }
+                o3 = a.f3[gi];
+                o4 = a.f4[gi];
+                sx = __ldg(a.abx + x);
+                sy = __ldg(a.aby + y);
+                sz = __ldg(a.abz + z);
+            }
+            // buoyancy-scaled first derivatives of plane z on the halo'd tile
+            for (int e = tid; e < 2 * TY * IW; e += NT) {
+                const int f = e / (TY * IW), r = (e / IW) % TY, c = e % IW;
+                const float* Pf = O1 + f * PH * PW;
+                const int gx = x0 - 4 + c;
+                float acc = 0.0f;
+#pragma unroll
+                for (int i = 1; i <= 4; ++i) acc += c1(i) * (Pf[(r + 8) * PW + c + 3 + i] - Pf[(r + 8) * PW + c + 4 - i]);
+                acc *= a.invdx;
+                const float v = acc * I7[(r + 4) * IW + c];
+                dxs[e] = (gx >= L.ixbeg && gx <= L.ixend) ? v : 0.0f;
+            }
+            for (int e = tid; e < 2 * IH * TX; e += NT) {
+                const int f = e / (IH * TX), r = (e / TX) % IH, c = e % TX;
+                const float* Pf = O1 + f * PH * PW;
+                const int gy = y0 - 4 + r;
+                float acc = 0.0f;
+#pragma unroll
+                for (int i = 1; i <= 4; ++i)
+                    acc += c1(i) * (Pf[(r + 3 + i) * PW + c + 8] - Pf[(r + 4 - i) * PW + c + 8]);
+                acc *= a.invdy;
+                const float v = acc * I7[r * IW + c + 4];
+                dys[e] = (gy >= L.iybeg && gy <= L.iyend) ? v : 0.0f;
+            }
+            __syncthreads();
+            if (owner) {
+                float xx1 = 0, xx2 = 0, yy1 = 0, yy2 = 0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    xx1 += tap(k) * dxs[ty * IW + tx + 1 + k];
+                    xx2 += tap(k) * dxs[TY * IW + ty * IW + tx + 1 + k];
+                    yy1 += tap(k) * dys[(ty + 1 + k) * TX + tx];
+                    yy2 += tap(k) * dys[IH * TX + (ty + 1 + k) * TX + tx];
+                }
+                xx1 *= a.invdx;
+                xx2 *= a.invdx;
+                yy1 *= a.invdy;
+                yy2 *= a.invdy;
+                float q1[8], q2[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    q1[j] = dZ1[j];
+                    q2[j] = dZ2[j];
+                }
+                if (a.fs) {
+                    resolve_dz(q1, z - L.izbeg);
+                    resolve_dz(q2, z - L.izbeg);
+                }
+                float zz1 = 0, zz2 = 0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    zz1 = zz1 + tap(k) * q1[k];
+                    zz2 = zz2 + tap(k) * q2[k];
+                }
+                zz1 *= a.invdz;
+                zz2 *= a.invdz;
+                const float ir = I7[(ty + 4) * IW + tx + 4];
+                const float rho = 1.0f / ir;
+                float r3, r4;
+                const float* O2 = O1 + PH * PW;
+                if constexpr (TTI) {
+                    float xy1 = 0, xy2 = 0;
+#pragma unroll
+                    for (int k = -4; k <= 4; ++k) {
+                        if (k == 0) continue;
+                        const float c = c2(k < 0 ? -k : k);
+                        xy1 += c * (O1[(vr + k) * PW + vc + k] - O1[(vr - k) * PW + vc + k]);
+                        xy2 += c * (O2[(vr + k) * PW + vc + k] - O2[(vr - k) * PW + vc + k]);
+                    }
+                    xy1 *= a.invdxdy;
+                    xy2 *= a.invdxdy;
+                    const float zx1 = mq[0][0], zx2 = mq[0][1], yz1 = mq[0][2], yz2 = mq[0][3];
+                    const float rx2 = vrx * vrx, ry2 = vry * vry, rz2 = vrz * vrz;
+                    const float rxy = 2.0f * vrx * vry, ryz = 2.0f * vry * vrz, rzx = 2.0f * vrz * vrx;
+                    xx1 *= rho;
+                    yy1 *= rho;
+                    zz1 *= rho;
+                    xx2 *= rho;
+                    yy2 *= rho;
+                    zz2 *= rho;
+                    const float V1 = rx2 * xx1 + ry2 * yy1 + rz2 * zz1 + rxy * xy1 + rzx * zx1 + ryz * yz1;
+                    const float H1 = xx1 + yy1 + zz1 - V1;
+                    const float V2 = rx2 * xx2 + ry2 * yy2 + rz2 * zz2 + rxy * xy2 + rzx * zx2 + ryz * yz2;
+                    const float H2 = xx2 + yy2 + zz2 - V2;
+                    r3 = a1 * H1 + a4 * V1 + a2 * V2;
+                    r4 = a2 * H1 + a3 * V2 + a4 * H2;
+                } else {
+                    // rx = ry = 0, rz = 1: V = zz exactly, H = xx + yy + zz - zz.
+                    xx1 *= rho;
+                    yy1 *= rho;
+                    zz1 *= rho;
+                    xx2 *= rho;
+                    yy2 *= rho;
+                    zz2 *= rho;
+                    const float V1 = zz1, V2 = zz2;
+                    const float H1 = xx1 + yy1 + zz1 - V1;
+                    const float H2 = xx2 + yy2 + zz2 - V2;
+                    r3 = a1 * H1 + a4 * V1 + a2 * V2;
+                    r4 = a2 * H1 + a3 * V2 + a4 * H2;
+                }
+                float n3 = o3 + r3 * a.dt;
+                float n4 = o4 + r4 * a.dt;
+                if (gi == a.src_index) {
+                    n3 += a.src_term;
+                    n4 += a.src_term;
+                }
+                a.f3[gi] = n3;
+                a.f4[gi] = n4;
+                const float pc = O1[vr * PW + vc], qc = O2[vr * PW + vc];
+                if (a.snap) {
+                    const int64_t nin = (int64_t)L.nx() * L.ny() * L.nz();
+                    const int64_t d = ((int64_t)(z - L.izbeg) * L.ny() + (y - L.iybeg)) * L.nx() + (x - L.ixbeg);
+                    a.snap[d] = n3;
+                    a.snap[nin + d] = n4;
+                    a.snap[2 * nin + d] = pc;
+                    a.snap[3 * nin + d] = qc;
+                }
+                // next step's loop2 (kernel_base.cu:92-101) and free surface (:142-162)
+                const float A = fminf(sx.x, fminf(sy.x, sz.x));
+                const float B = fminf(sx.y, fminf(sy.y, sz.y));
+                float np = A * pc + B * n3 * a.dt;
+                float nq = A * qc + B * n4 * a.dt;
+                if (a.fs && z == L.izbeg) {
+                    np = 0.0f;
+                    nq = 0.0f;
+                }
+                a.pout[gi] = np;
+                a.qout[gi] = nq;
+                if (a.fs && z > L.izbeg && z <= L.izbeg + kRadius) {
+                    const int64_t gm = L.idx(x, y, 2 * L.izbeg - z);
+                    a.pout[gm] = -np;
+                    a.qout[gm] = -nq;
+                }
+            }
+        }
+        if constexpr (TTI) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                mq[0][c] = mq[1][c];
+                mq[1][c] = mq[2][c];
+                mq[2][c] = mz[c];
+            }
+        }
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Fused adjoint step (one reference adjoint step: adj_drv, loop4_derivatives,
+// update_adj_kernel_main_3, loop2, loop4).  The transposed model is applied
+// before the derivatives (kernel_type2_grad_snap.cu:98-129), so every term of
+// an output cell is a plain sum and the terms are accumulated in per-thread
+// queues as the planes arrive: the x+y part when plane z arrives, the mixed
+// part plane by plane from z-4 to z+4 (the reference's order), the z part when
+// plane z+7 arrives.
+struct AdjParams {
+    float* pout;
+    float* qout;
+    float* f3;
+    float* f4;
+    const float* pin;
+    const float* qin;
+    const float2 *abx, *aby, *abz;
+    Layout L;
+    int bz;
+    int fs;
+    int sponge;
+    float dt, invdx, invdy, invdz, invdxy, invdyz, invdzx;
+    int* err;
+};
+
+// Staging per plane: p, q, m1, m2, m3, m4, irho, rx, ry with a halo of 8 and
+// rz with a halo of 4.
+constexpr int ADJ_NSTAGE = 3;
+constexpr int ADJ_PF = 2;
+constexpr int ADJ_NARR = 9;
+constexpr size_t ADJ_ARR = (size_t)PH * PW * sizeof(float);
+constexpr size_t ADJ_RZ = (size_t)IH * IW * sizeof(float);
+constexpr size_t ADJ_STAGE = ADJ_NARR * ADJ_ARR + ADJ_RZ;
+constexpr size_t ADJ_TXX = (size_t)2 * TY * PW * sizeof(float);  // rows y0.., cols x0-8..
+constexpr size_t ADJ_TYY = (size_t)2 * PH * TX * sizeof(float);  // rows y0-8.., cols x0..
+constexpr size_t ADJ_TXY = (size_t)2 * IH * IW * sizeof(float);  // rows y0-4.., cols x0-4..
+constexpr size_t ADJ_TYZ = (size_t)2 * IH * TX * sizeof(float);  // rows y0-4.., cols x0..
+constexpr size_t ADJ_TZX = (size_t)2 * TY * IW * sizeof(float);  // rows y0.., cols x0-4..
+constexpr size_t ADJ_DX = (size_t)2 * TY * IW * sizeof(float);   // rows y0.., cols x0-4..
+constexpr size_t ADJ_DY = (size_t)2 * IH * TX * sizeof(float);   // rows y0-4.., cols x0..
+constexpr size_t ADJ_SMEM = ADJ_NSTAGE * ADJ_STAGE + ADJ_TXX + ADJ_TYY + ADJ_TXY + ADJ_TYZ + ADJ_TZX + ADJ_DX +
+                            ADJ_DY + ADJ_NSTAGE * sizeof(uint64_t);
+
+struct AdjMaps {
+    CUtensorMap m[ADJ_NARR];  // p, q, m1, m2, m3, m4, irho, rx, ry  (box PW x PH)
+    CUtensorMap rz;           // box IW x IH
+};
+
+enum { S_P = 0, S_Q, S_M1, S_M2, S_M3, S_M4, S_IR, S_RX, S_RY };
+
+// Point-wise transposed model at staging offset k:
+//   s1 = m1 p + m2 q, h1 = (-m1 + m4) p - m2 q, s2 = m4 q, h2 = m2 p + (-m4 + m3) q.
+struct Base {
+    float s1, h1, s2, h2, rho;
+};
+__device__ __forceinline__ Base base_at(const float* st, int k)
+{
+    const float p = st[S_P * PH * PW + k], q = st[S_Q * PH * PW + k];
+    const float a1 = st[S_M1 * PH * PW + k], a2 = st[S_M2 * PH * PW + k], a3 = st[S_M3 * PH * PW + k],
+                a4 = st[S_M4 * PH * PW + k];
+    Base b;
+    b.s1 = a1 * p + a2 * q;
+    b.h1 = (-a1 + a4) * p - a2 * q;
+    b.s2 = a4 * q;
+    b.h2 = a2 * p + (-a4 + a3) * q;
+    b.rho = 1.0f / st[S_IR * PH * PW + k];
+    return b;
+}
+
+template <bool TTI>
+__global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__ AdjMaps tm, const AdjParams a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* stage = reinterpret_cast<float*>(smem);
+    unsigned char* sp = smem + ADJ_NSTAGE * ADJ_STAGE;
+    float* txx = reinterpret_cast<float*>(sp);
+    sp += ADJ_TXX;
+    float* tyy = reinterpret_cast<float*>(sp);
+    sp += ADJ_TYY;
+    float* txy = reinterpret_cast<float*>(sp);
+    sp += ADJ_TXY;
+    float* tyz = reinterpret_cast<float*>(sp);
+    sp += ADJ_TYZ;
+    float* tzx = reinterpret_cast<float*>(sp);
+    sp += ADJ_TZX;
+    float* dxs = reinterpret_cast<float*>(sp);
+    sp += ADJ_DX;
+    float* dys = reinterpret_cast<float*>(sp);
+    sp += ADJ_DY;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sp);
+
+    const Layout& L = a.L;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int x0 = L.ixbeg + blockIdx.x * TX, y0 = L.iybeg + blockIdx.y * TY;
+    const int zs = L.izbeg + blockIdx.z * a.bz;
+    const int ze = min(zs + a.bz - 1, L.izend);
+    const int ntot = ze - zs + 1 + 2 * LAG;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool owner = (x <= L.ixend) && (y <= L.iyend);
+    bool dead = false;
+    constexpr int NLOAD = TTI ? ADJ_NARR : S_RX;  // VTI: rx, ry, rz are not read
+    constexpr uint32_t TX_BYTES = (uint32_t)(NLOAD * ADJ_ARR + (TTI ? ADJ_RZ : 0));
+
+    if (tid == 0) {
+        for (int s = 0; s < ADJ_NSTAGE; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int t) {
+        const int s = t % ADJ_NSTAGE, z = zs - LAG + t;
+        float* dst = stage + (size_t)s * (ADJ_STAGE / sizeof(float));
+        mbar_expect_tx(&bars[s], TX_BYTES);
+#pragma unroll
+        for (int k = 0; k < NLOAD; ++k) tma_load_3d(dst + k * PH * PW, &tm.m[k], x0 - 8, y0 - 8, z, &bars[s]);
+        if constexpr (TTI) tma_load_3d(dst + ADJ_NARR * PH * PW, &tm.rz, x0 - 4, y0 - 4, z, &bars[s]);
+    };
+    if (tid == 0)
+        for (int t = 0; t < ADJ_PF && t < ntot; ++t) issue(t);
+
+    float dzq1[8], dzq2[8];  // D- partial sums, positions L-3 .. L+4
+    float dZ1[8], dZ2[8];    // buoyancy-scaled z derivatives, positions L-10 .. L-3
+    float mx1[12], mx2[12];  // mixed rhs, outputs L-7 .. L+4
+    float sxy1[8], sxy2[8];  // x+y parts, outputs L-7 .. L
+    float irq[4];            // buoyancy of this column, planes L-3 .. L
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dzq1[j] = dzq2[j] = dZ1[j] = dZ2[j] = sxy1[j] = sxy2[j] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 12; ++j) mx1[j] = mx2[j] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) irq[j] = 0.0f;
+
+    for (int t = 0; t < ntot; ++t) {
+        // Stage (t+2)%3 was last read in iteration t-1, before its final barrier.
+        if (tid == 0 && t + ADJ_PF < ntot) {
+            fence_proxy_async();
+            issue(t + ADJ_PF);
+        }
+        const int s = t % ADJ_NSTAGE;
+        const int Lz = zs - LAG + t;
+        mbar_wait(&bars[s], (uint32_t)((t / ADJ_NSTAGE) & 1), a.err, dead);
+        const float* st = stage + (size_t)s * (ADJ_STAGE / sizeof(float));
+        const float* srz = st + ADJ_NARR * PH * PW;  // rz tile, origin (x0-4, y0-4)
+
+        // (1) temporaries of plane L
+        for (int e = tid; e < TY * PW; e += NT) {  // xx: rows y0.., cols x0-8..
+            const int r = e / PW, c = e % PW;
+            const int k = (r + 8) * PW + c;
+            const Base b = base_at(st, k);
+            const float vr = TTI ? st[S_RX * PH * PW + k] : 0.0f;
+            const float rr = vr * vr;
+            txx[e] = b.rho * (b.s1 + rr * b.h1);
+            txx[TY * PW + e] = b.rho * (b.s2 + rr * b.h2);
+        }
+        for (int e = tid; e < PH * TX; e += NT) {  // yy: rows y0-8.., cols x0..
+            const int r = e / TX, c = e % TX;
+            const int k = r * PW + c + 8;
+            const Base b = base_at(st, k);
+            const float vr = TTI ? st[S_RY * PH * PW + k] : 0.0f;
+            const float rr = vr * vr;
+            tyy[e] = b.rho * (b.s1 + rr * b.h1);
+            tyy[PH * TX + e] = b.rho * (b.s2 + rr * b.h2);
+        }
+        if constexpr (TTI) {
+            for (int e = tid; e < IH * IW; e += NT) {  // xy: rows y0-4.., cols x0-4..
+                const int r = e / IW, c = e % IW;
+                const int k = (r + 4) * PW + c + 4;
+                const Base b = base_at(st, k);
+                const float w = 2.0f * st[S_RX * PH * PW + k] * st[S_RY * PH * PW + k];
+                txy[e] = w * b.h1;
+                txy[IH * IW + e] = w * b.h2;
+            }
+            for (int e = tid; e < IH * TX; e += NT) {  // yz: rows y0-4.., cols x0..
+                const int r = e / TX, c = e % TX;
+                const int k = (r + 4) * PW + c + 8;
+                const Base b = base_at(st, k);
+                const float w = 2.0f * st[S_RY * PH * PW + k] * srz[r * IW + c + 4];
+                tyz[e] = w * b.h1;
+                tyz[IH * TX + e] = w * b.h2;
+            }
+            for (int e = tid; e < TY * IW; e += NT) {  // zx: rows y0.., cols x0-4..
+                const int r = e / IW, c = e % IW;
+                const int k = (r + 8) * PW + c + 4;
+                const Base b = base_at(st, k);
+                const float w = 2.0f * srz[(r + 4) * IW + c] * st[S_RX * PH * PW + k];
+                tzx[e] = w * b.h1;
+                tzx[TY * IW + e] = w * b.h2;
+            }
+        }
+        // this column's zz temporary and buoyancy at plane L
+        const int kc = (ty + 8) * PW + tx + 8;
+        float tz1, tz2;
+        {
+            const Base b = base_at(st, kc);
+            const float vr = TTI ? srz[(ty + 4) * IW + tx + 4] : 1.0f;
+            const float rr = vr * vr;
+            tz1 = b.rho * (b.s1 + rr * b.h1);
+            tz2 = b.rho * (b.s2 + rr * b.h2);
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) irq[j] = irq[j + 1];
+        irq[3] = st[S_IR * PH * PW + kc];
+        __syncthreads();  // temporaries of plane L are ready
+
+        // (2) buoyancy-scaled x/y derivatives of plane L (compute_xy_contributions)
+        for (int e = tid; e < 2 * TY * IW; e += NT) {
+            const int f = e / (TY * IW), r = (e / IW) % TY, c = e % IW;  // x = x0-4+c, y = y0+r
+            const float* T = txx + f * TY * PW + r * PW;
+            const float irv = st[S_IR * PH * PW + (r + 8) * PW + c + 4];
+            float acc = 0.0f;
+#pragma unroll
+            for (int i = 1; i <= 4; ++i) acc += (a.invdx * c1(i)) * (T[c + 3 + i] - T[c + 4 - i]) * irv;
+            const int gx = x0 - 4 + c;
+            dxs[e] = (gx >= L.ixbeg && gx <= L.ixend) ? acc : 0.0f;
+        }
+        for (int e = tid; e < 2 * IH * TX; e += NT) {
+            const int f = e / (IH * TX), r = (e / TX) % IH, c = e % TX;  // y = y0-4+r, x = x0+c
+            const float* T = tyy + f * PH * TX;
+            const float irv = st[S_IR * PH * PW + (r + 4) * PW + c + 8];
+            float acc = 0.0f;
+#pragma unroll
+            for (int i = 1; i <= 4; ++i)
+                acc += (a.invdy * c1(i)) * (T[(r + 3 + i) * TX + c] - T[(r + 4 - i) * TX + c]) * irv;
+            const int gy = y0 - 4 + r;
+            dys[e] = (gy >= L.iybeg && gy <= L.iyend) ? acc : 0.0f;
+        }
+        // (3) D- z stage (compute_z_contributionsdtd), completes position L-3
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float alpha = (j <= 3) ? a.invdz * c1(4 - j) : -a.invdz * c1(j - 3);
+            dzq1[j] = dzq1[j] + alpha * tz1;
+            dzq2[j] = dzq2[j] + alpha * tz2;
+        }
+        {
+            const int zp = Lz - 3;
+            const bool valid = (zp >= L.izbeg + (a.fs ? 1 : 0)) && zp <= L.izend;
+            const float n1 = valid ? dzq1[0] * irq[0] : 0.0f;
+            const float n2 = valid ? dzq2[0] * irq[0] : 0.0f;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) {
+                dZ1[j] = dZ1[j + 1];
+                dZ2[j] = dZ2[j + 1];
+                dzq1[j] = dzq1[j + 1];
+                dzq2[j] = dzq2[j + 1];
+            }
+            dZ1[7] = n1;
+            dZ2[7] = n2;
+            dzq1[7] = 0.0f;
+            dzq2[7] = 0.0f;
+        }
+        // (4) mixed rhs: scatter of plane L into outputs L-4 .. L+4, then xy into output L
+        if constexpr (TTI) {
+            const float* Y1 = tyz;
+            const float* Y2 = tyz + IH * TX;
+            const float* Z1 = tzx;
+            const float* Z2 = tzx + TY * IW;
+#pragma unroll
+            for (int ir = -4; ir <= 4; ++ir) {
+                if (ir == 0) continue;
+                const float c = c2(ir < 0 ? -ir : ir);
+                const int j = 7 - ir;  // output L - ir
+                const float t1 = (a.invdyz * c) * (Y1[(ty + 4 + ir) * TX + tx] - Y1[(ty + 4 - ir) * TX + tx]);
+                const float t2 = (a.invdzx * c) * (Z1[ty * IW + tx + 4 + ir] - Z1[ty * IW + tx + 4 - ir]);
+                const float u1 = (a.invdyz * c) * (Y2[(ty + 4 + ir) * TX + tx] - Y2[(ty + 4 - ir) * TX + tx]);
+                const float u2 = (a.invdzx * c) * (Z2[ty * IW + tx + 4 + ir] - Z2[ty * IW + tx + 4 - ir]);
+                mx1[j] = mx1[j] + t1 + t2;
+                mx2[j] = mx2[j] + u1 + u2;
+            }
+            const float* T2 = txy + IH * IW;
+            const int cc = tx + 4, rr = ty + 4;
+            float s3 = mx1[7], s4 = mx2[7];
+#pragma unroll
+            for (int k = 1; k <= 4; ++k) {
+                const float axy = a.invdxy * c2(k);
+                s3 += axy * (txy[(rr + k) * IW + cc + k] - txy[(rr + k) * IW + cc - k] + txy[(rr - k) * IW + cc - k] -
+                             txy[(rr - k) * IW + cc + k]);
+                s4 += axy * (T2[(rr + k) * IW + cc + k] - T2[(rr + k) * IW + cc - k] + T2[(rr - k) * IW + cc - k] -
+                             T2[(rr - k) * IW + cc + k]);
+            }
+            mx1[7] = s3;
+            mx2[7] = s4;
+        }
+        __syncthreads();  // dxs/dys of plane L are ready
+
+        // (5) x+y parts of output L (dfdx_stg_right, kernel_type2_adj.cu:85-98)
+        {
+            float sx1 = 0, sx2 = 0, sy1 = 0, sy2 = 0;
+            const float* X2 = dxs + TY * IW;
+            const float* Y2 = dys + IH * TX;
+#pragma unroll
+            for (int k = 1; k <= 4; ++k) {
+                sx1 += c1(k) * (dxs[ty * IW + tx + 4 + k] - dxs[ty * IW + tx + 5 - k]);
+                sx2 += c1(k) * (X2[ty * IW + tx + 4 + k] - X2[ty * IW + tx + 5 - k]);
+                sy1 += c1(k) * (dys[(ty + 4 + k) * TX + tx] - dys[(ty + 5 - k) * TX + tx]);
+                sy2 += c1(k) * (Y2[(ty + 4 + k) * TX + tx] - Y2[(ty + 5 - k) * TX + tx]);
+            }
+            sx1 *= a.invdx;
+            sx2 *= a.invdx;
+            sy1 *= a.invdy;
+            sy2 *= a.invdy;
+            sxy1[7] = sx1 + sy1;
+            sxy2[7] = sx2 + sy2;
+        }
+        // (6) output plane L-7
+        const int z = Lz - LAG;
+        if (z >= zs && owner) {
+            const int64_t gi = L.idx(x, y, z);
+            float q1[8], q2[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                q1[j] = dZ1[j];
+                q2[j] = dZ2[j];
+            }
+            if (a.fs) {
+                resolve_dz(q1, z - L.izbeg);
+                resolve_dz(q2, z - L.izbeg);
+            }
+            float sz1 = 0, sz2 = 0;
+#pragma unroll
+            for (int k = 1; k <= 4; ++k) {
+                sz1 += c1(k) * (q1[3 + k] - q1[4 - k]);
+                sz2 += c1(k) * (q2[3 + k] - q2[4 - k]);
+            }
+            sz1 *= a.invdz;
+            sz2 *= a.invdz;
+            float r3 = sxy1[0] + sz1;
+            float r4 = sxy2[0] + sz2;
+            r3 += mx1[0];
+            r4 += mx2[0];
+            const float2 sx = __ldg(a.abx + x), sy = __ldg(a.aby + y), sz = __ldg(a.abz + z);
+            const float o3 = a.f3[gi], o4 = a.f4[gi];
+            float n3, n4;
+            if (a.sponge) {
+                const float A = fminf(fminf(sx.x, sy.x), sz.x);
+                const float B = fminf(fminf(sx.y, sy.y), sz.y) * a.dt;
+                n3 = A * o3 + B * r3;
+                n4 = A * o4 + B * r4;
+            } else {
+                n3 = o3 + r3 * a.dt;
+                n4 = o4 + r4 * a.dt;
+            }
+            a.f3[gi] = n3;
+            a.f4[gi] = n4;
+            // loop2 (kernel_base.cu:92-101) and free surface (:142-162)
+            const float A = fminf(sx.x, fminf(sy.x, sz.x));
+            const float B = fminf(sx.y, fminf(sy.y, sz.y));
+            const float pc = __ldg(a.pin + gi), qc = __ldg(a.qin + gi);
+            float np = A * pc + B * n3 * a.dt;
+            float nq = A * qc + B * n4 * a.dt;
+            if (a.fs && z == L.izbeg) {
+                np = 0.0f;
+                nq = 0.0f;
+            }
+            a.pout[gi] = np;
+            a.qout[gi] = nq;
+            if (a.fs && z > L.izbeg && z <= L.izbeg + kRadius) {
+                const int64_t gm = L.idx(x, y, 2 * L.izbeg - z);
+                a.pout[gm] = -np;
+                a.qout[gm] = -nq;
+            }
+        }
+        // (7) rotate the output queues
+#pragma unroll
+        for (int j = 0; j < 7; ++j) {
+            sxy1[j] = sxy1[j + 1];
+            sxy2[j] = sxy2[j + 1];
+        }
+#pragma unroll
+        for (int j = 0; j < 11; ++j) {
+            mx1[j] = mx1[j + 1];
+            mx2[j] = mx2[j + 1];
+        }
+        mx1[11] = 0.0f;
+        mx2[11] = 0.0f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: tensor maps and launchers.
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// 3D FP32 tensor map over a halo'd volume with a (bx, by, 1) box; reads
+// outside the volume are zero-filled.
+bool make_map(CUtensorMap* m, const float* base, const Layout& L, int bx, int by)
+{
+    auto fn = encode_fn();
+    if (!fn || !base) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)L.ldimx, (cuuint64_t)L.ldimy, (cuuint64_t)L.ldimz};
+    cuuint64_t strides[2] = {(cuuint64_t)L.ldimx * sizeof(float), (cuuint64_t)L.ldimx * L.ldimy * sizeof(float)};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// Maps are keyed by (address, box, layout) and cached for the process.
+struct MapKey {
+    const float* p;
+    int bx, by, lx, ly, lz;
+    bool operator<(const MapKey& o) const
+    {
+        return std::tie(p, bx, by, lx, ly, lz) < std::tie(o.p, o.bx, o.by, o.lx, o.ly, o.lz);
+    }
+};
+std::mutex g_map_mu;
+std::map<MapKey, CUtensorMap> g_maps;
+
+bool get_map(CUtensorMap* out, const float* p, const Layout& L, int bx, int by)
+{
+    MapKey k{p, bx, by, L.ldimx, L.ldimy, L.ldimz};
+    std::lock_guard<std::mutex> lk(g_map_mu);
+    auto it = g_maps.find(k);
+    if (it != g_maps.end()) {
+        *out = it->second;
+        return true;
+    }
+    CUtensorMap m;
+    if (!make_map(&m, p, L, bx, by)) return false;
+    if (g_maps.size() > 4096) g_maps.clear();
+    g_maps[k] = m;
+    *out = m;
+    return true;
+}
+
+// Per-device error word for the bounded waits.
+int* err_word()
+{
+    static std::mutex mu;
+    static std::map<int, int*> words;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = words.find(dev);
+    if (it != words.end()) return it->second;
+    int* p = nullptr;
+    if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaMemset(p, 0, sizeof(int));
+    words[dev] = p;
+    return p;
+}
+
+bool layout_supported(const Layout& L)
+{
+    // TMA box origins x0-8 and x0-4 must be multiples of 4 floats (16 bytes):
+    // ixbeg = 4 and a 32-wide tile guarantee it.
+    return L.ixbeg == kRadius && L.iybeg == kRadius && L.izbeg == kRadius && L.ldimx % 32 == 0 &&
+           L.ldimx >= L.ixend + 1 + kRadius && L.ldimy == L.iyend + 1 + kRadius &&
+           L.ldimz == L.izend + 1 + kRadius;
+}
+
+int pick_bz(const Layout& L)
+{
+    // Enough CTAs to fill the 148 SMs at one CTA per SM; longer chunks
+    // amortise the 14-plane pipeline fill.
+    const int tiles = ((L.nx() + TX - 1) / TX) * ((L.ny() + TY - 1) / TY);
+    int bz = L.nz();
+    while (bz > 32 && (long)tiles * ((L.nz() + bz - 1) / bz) < 2 * 148) bz = (bz + 1) / 2;
+    return bz;
+}
+
+} // namespace
+
+int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
+{
+    if (!layout_supported(L)) return TTI_EINVAL;
+    CUtensorMap mp, mq, mi;
+    if (!get_map(&mp, s.pin, L, PW, PH) || !get_map(&mq, s.qin, L, PW, PH) || !get_map(&mi, s.m.irho, L, IW, IH))
+        return TTI_ELAUNCH;
+    FwdParams a{};
+    a.pout = s.pout;
+    a.qout = s.qout;
+    a.f3 = s.f3;
+    a.f4 = s.f4;
+    a.irho = s.m.irho;
+    a.m1 = s.m.m1;
+    a.m2 = s.m.m2;
+    a.m3 = s.m.m3;
+    a.m4 = s.m.m4;
+    a.rx = s.m.rx;
+    a.ry = s.m.ry;
+    a.rz = s.m.rz;
+    a.abx = s.abx;
+    a.aby = s.aby;
+    a.abz = s.abz;
+    a.snap = s.snap;
+    a.src_index = s.src_index;
+    a.src_term = s.src_term;
+    a.L = L;
+    a.bz = pick_bz(L);
+    a.fs = s.free_surface;
+    a.dt = s.dt;
+    a.invdx = 1.0 / s.dx;
+    a.invdy = 1.0 / s.dy;
+    a.invdz = 1.0 / s.dz;
+    a.invdxdy = 1.0 / (4 * s.dx * s.dy);
+    a.invdydz = 1.0 / (4 * s.dy * s.dz);
+    a.invdzdx = 1.0 / (4 * s.dx * s.dz);
+    a.err = err_word();
+    if (!a.err) return TTI_ENOMEM;
+    dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
+    static bool attr_set[2] = {false, false};
+    if (s.vti) {
+        if (!attr_set[0]) {
+            cudaFuncSetAttribute(k_fused_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM);
+            attr_set[0] = true;
+        }
+        k_fused_forward<false><<<grid, dim3(TX, TY), FWD_SMEM, st>>>(mp, mq, mi, a);
+    } else {
+        if (!attr_set[1]) {
+            cudaFuncSetAttribute(k_fused_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM);
+            attr_set[1] = true;
+        }
+        k_fused_forward<true><<<grid, dim3(TX, TY), FWD_SMEM, st>>>(mp, mq, mi, a);
+    }
+    return launch_status();
+}
+
+int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
+{
+    if (!layout_supported(L)) return TTI_EINVAL;
+    AdjMaps tm;
+    const float* arr[ADJ_NARR] = {s.pin, s.qin, s.m.m1, s.m.m2, s.m.m3, s.m.m4, s.m.irho, s.m.rx, s.m.ry};
+    for (int k = 0; k < ADJ_NARR; ++k)
+        if (!get_map(&tm.m[k], arr[k], L, PW, PH)) return TTI_ELAUNCH;
+    if (!get_map(&tm.rz, s.m.rz, L, IW, IH)) return TTI_ELAUNCH;
+    AdjParams a{};
+    a.pout = s.pout;
+    a.qout = s.qout;
+    a.f3 = s.f3;
+    a.f4 = s.f4;
+    a.pin = s.pin;
+    a.qin = s.qin;
+    a.abx = s.abx;
+    a.aby = s.aby;
+    a.abz = s.abz;
+    a.L = L;
+    a.bz = pick_bz(L);
+    a.fs = s.free_surface;
+    a.sponge = s.sponge_active;
+    a.dt = s.dt;
+    a.invdx = 1.0 / s.dx;
+    a.invdy = 1.0 / s.dy;
+    a.invdz = 1.0 / s.dz;
+    a.invdxy = 1.0 / (4 * s.dx * s.dy);
+    a.invdyz = 1.0 / (4 * s.dy * s.dz);
+    a.invdzx = 1.0 / (4 * s.dx * s.dz);
+    a.err = err_word();
+    if (!a.err) return TTI_ENOMEM;
+    const bool tti = !s.vti;
+    dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
+    static bool attr_set[2] = {false, false};
+    if (!tti) {
+        if (!attr_set[0]) {
+            cudaFuncSetAttribute(k_fused_adjoint<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
+            attr_set[0] = true;
+        }
+        k_fused_adjoint<false><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
+    } else {
+        if (!attr_set[1]) {
+            cudaFuncSetAttribute(k_fused_adjoint<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
+            attr_set[1] = true;
+        }
+        k_fused_adjoint<true><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
+    }
+    return launch_status();
+}
+
+// Bounded-wait status of the fused kernels on the current device: 0 if no
+// wait gave up since the last call; the word is cleared.
+int fused_wait_status(cudaStream_t st)
+{
+    int* w = err_word();
+    if (!w) return TTI_ENOMEM;
+    int h = 0;
+    if (cudaMemcpyAsync(&h, w, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return TTI_ELAUNCH;
+    }
+    if (h) {
+        cudaMemsetAsync(w, 0, sizeof(int), st);
+        return TTI_ETIMEOUT;
+    }
+    return TTI_OK;
+}
+
+} // namespace tti

@@ -1,0 +1,77 @@
+// Internal launch helpers shared by the simulator, the C ABI and the fused
+// kernels.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "tti_common.cuh"
+
+namespace tti {
+
+int launch_base(const float* f1, const float* f2, const float* m1, const float* m2, const float* m3,
+                const float* m4, float4* base, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+                int ldimx, int ldimy, cudaStream_t st);
+int launch_adj_drv_with_base(float* d1x, float* d2x, float* d1y, float* d2y, float* d1z, float* d2z, float* rhs3,
+                             float* rhs4, const float4* base, const float* irho, const float* rx, const float* ry,
+                             const float* rz, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+                             int ldimx, int ldimy, float invdxy, float invdyz, float invdzx, float invdx, float invdy,
+                             float invdz, cudaStream_t st);
+int launch_rho_gradient_with_base(float* grad, const float* fd1x, const float* fd2x, const float* fd1y,
+                                  const float* fd2y, const float* fd1z, const float* fd2z, const float4* base,
+                                  const float* irho, const float* rx, const float* ry, const float* rz, int ixbeg,
+                                  int ixend, int iybeg, int iyend, int izbeg, int izend, int ldimx, int ldimy,
+                                  int gldx, int gldy, double dx, double dy, double dz, cudaStream_t st);
+
+// Model volumes in the reference layout, all halo'd.
+struct Model {
+    const float *irho, *m1, *m2, *m3, *m4, *rx, *ry, *rz;
+};
+
+// Fused forward step (tti_fused.cu).  Reads p,q at time n from pin/qin
+// (free surface already applied), updates pdot/qdot in place with the TTI
+// operator plus the point source, writes p,q at time n+1 (loop2 + free
+// surface) to pout/qout, and optionally stores the snapshot of this step.
+struct FwdStepArgs {
+    const float* pin;
+    const float* qin;
+    float* pout;
+    float* qout;
+    float* f3;
+    float* f4;
+    Model m;
+    const float2 *abx, *aby, *abz;
+    int64_t src_index;  // -1: no source
+    float src_term;     // w[n]*dt
+    float* snap;        // nullptr or 4 interior volumes: pdot, qdot, p, q
+    int free_surface;
+    int vti;            // 1: rx=ry=0, rz=1 are not read
+    float dt;
+    double dx, dy, dz;
+};
+int launch_fused_forward(const Layout& L, const FwdStepArgs& a, cudaStream_t st);
+
+// Fused adjoint step (tti_fused.cu): the reference's adjoint sequence
+// adj_drv, loop4_derivatives, adj_update, loop2, loop4 in one pass.
+struct AdjStepArgs {
+    const float* pin;
+    const float* qin;
+    float* pout;
+    float* qout;
+    float* f3;
+    float* f4;
+    Model m;
+    const float2 *abx, *aby, *abz;
+    int sponge_active;
+    int free_surface;
+    int vti;
+    float dt;
+    double dx, dy, dz;
+};
+int launch_fused_adjoint(const Layout& L, const AdjStepArgs& a, cudaStream_t st);
+
+// Status of the bounded waits inside the fused kernels since the last call
+// (TTI_ETIMEOUT if any gave up); synchronizes the stream.
+int fused_wait_status(cudaStream_t st);
+
+} // namespace tti

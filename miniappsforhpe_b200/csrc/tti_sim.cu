@@ -1,0 +1,834 @@
+// Simulator object: the simulator2SetUp call surface on one B200.
+//
+// Mirrors simulator2/simulator2SetUp.{h,cu}: model setup (init_cijs plus the
+// buoyancy volume the reference never fills, simulator2SetUp.cu:476-502,
+// kernel_type2.cu:136-141), the forward time loop with snapshots every
+// xcorr_step steps (:530-651), the adjoint loop with the imaging condition
+// at snapshot steps (:654-782), and image readback.  Differences from the
+// reference, all deliberate:
+//   * one domain on one GPU: no zones, no halo exchange, no MPI;
+//   * snapshots stay in HBM (interior only; p/q halos are re-derived);
+//   * a point source injected every step and receivers sampled every step
+//     (the reference only seeds an impulse, simulator2SetUp.cu:44-49);
+//   * the adjoint starts from rest and is driven by residual traces;
+//   * the density gradient is stored interior-only at its own cells.
+// Every call returns a status code; nothing aborts.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "tti_common.cuh"
+#include "tti_internal.cuh"
+
+using namespace tti;
+
+namespace {
+
+// Interior (nx*ny*nz, x fastest) -> halo'd volume, halo by edge extension.
+__global__ void k_scatter_extend(float* __restrict__ vol, const float* __restrict__ in, Layout L)
+{
+    int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    int iy = blockIdx.y;
+    int iz = blockIdx.z;
+    if (ix >= L.ldimx) return;
+    int nx = L.nx(), ny = L.ny(), nz = L.nz();
+    int jx = min(max(ix - L.ixbeg, 0), nx - 1);
+    int jy = min(max(iy - L.iybeg, 0), ny - 1);
+    int jz = min(max(iz - L.izbeg, 0), nz - 1);
+    vol[L.idx(ix, iy, iz)] = in[((int64_t)jz * ny + jy) * nx + jx];
+}
+
+// Interior copy between a halo'd volume and a dense interior array.
+template <bool TO_DENSE>
+__global__ void k_interior_copy(float* __restrict__ vol, float* __restrict__ dense, Layout L)
+{
+    int jx = blockIdx.x * blockDim.x + threadIdx.x;
+    int jy = blockIdx.y;
+    int jz = blockIdx.z;
+    int nx = L.nx();
+    if (jx >= nx) return;
+    int64_t d = ((int64_t)jz * L.ny() + jy) * nx + jx;
+    int64_t v = L.idx(jx + L.ixbeg, jy + L.iybeg, jz + L.izbeg);
+    if (TO_DENSE)
+        dense[d] = vol[v];
+    else
+        vol[v] = dense[d];
+}
+
+// Snapshot of one forward step: pdot, qdot, p, q interior -> slot.
+__global__ void k_snapshot_save(float* __restrict__ slot, const float* __restrict__ f3, const float* __restrict__ f4,
+                                const float* __restrict__ f1, const float* __restrict__ f2, Layout L)
+{
+    int jx = blockIdx.x * blockDim.x + threadIdx.x;
+    int jy = blockIdx.y;
+    int jz = blockIdx.z;
+    int nx = L.nx();
+    if (jx >= nx) return;
+    int64_t n = (int64_t)nx * L.ny() * L.nz();
+    int64_t d = ((int64_t)jz * L.ny() + jy) * nx + jx;
+    int64_t v = L.idx(jx + L.ixbeg, jy + L.iybeg, jz + L.izbeg);
+    slot[d] = f3[v];
+    slot[n + d] = f4[v];
+    slot[2 * n + d] = f1[v];
+    slot[3 * n + d] = f2[v];
+}
+
+__global__ void k_add_source(float* f3, float* f4, int64_t i, float term)
+{
+    f3[i] += term;
+    f4[i] += term;
+}
+
+__global__ void k_receivers(float* __restrict__ out, const float* __restrict__ f1, const float* __restrict__ f2,
+                            const int64_t* __restrict__ rec, int nrec)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrec) return;
+    int64_t i = rec[r];
+    out[r] = -(2 * f1[i] + f2[i]) / 3;
+}
+
+// Adjoint p+q at the source cell: dt times this is the gradient of the
+// receiver misfit with respect to the source wavelet sample of that step.
+__global__ void k_source_trace(float* __restrict__ out, const float* __restrict__ f1, const float* __restrict__ f2,
+                               int64_t i)
+{
+    *out = f1[i] + f2[i];
+}
+
+// Residual injection: (-2/3, -1/3) times the residual, the transpose of the
+// pressure receiver -(2p+q)/3.  With obs != nullptr the residual is the
+// recorded synthetic trace minus the observed one.
+__global__ void k_inject_residual(float* __restrict__ f3, float* __restrict__ f4, const int64_t* __restrict__ rec,
+                                  const float* __restrict__ res, const float* __restrict__ obs, int nrec)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrec) return;
+    int64_t i = rec[r];
+    float v = obs ? res[r] - obs[r] : res[r];
+    f3[i] += (-2.0f / 3.0f) * v;
+    f4[i] += (-1.0f / 3.0f) * v;
+}
+
+// Interior-only Vp image scaling g *= -2*dt_xcorr/vp (kernel_type2_small.cu:61-74).
+__global__ void k_finalize_dense(float* __restrict__ g, const float* __restrict__ m3, Layout L, float dt_xcorr)
+{
+    int jx = blockIdx.x * blockDim.x + threadIdx.x;
+    int jy = blockIdx.y;
+    int jz = blockIdx.z;
+    int nx = L.nx();
+    if (jx >= nx) return;
+    int64_t d = ((int64_t)jz * L.ny() + jy) * nx + jx;
+    float vp = sqrtf(m3[L.idx(jx + L.ixbeg, jy + L.iybeg, jz + L.izbeg)]);
+    g[d] *= -dt_xcorr * 2.0 / vp;
+}
+
+inline int cuda_rc(cudaError_t e)
+{
+    if (e == cudaSuccess) return TTI_OK;
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? TTI_ENOMEM : TTI_ELAUNCH;
+}
+
+} // namespace
+
+struct tti_sim {
+    tti_sim_config cfg{};
+    Layout L{};
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    float *f1 = nullptr, *f2 = nullptr, *f3 = nullptr, *f4 = nullptr;
+    float *g1 = nullptr, *g2 = nullptr;  // second p/q buffers (fused steps)
+    float* d[6] = {};
+    float *rhs3 = nullptr, *rhs4 = nullptr;
+    float* mv[8] = {};  // irho, m1..m4, rx, ry, rz
+    float2 *abx = nullptr, *aby = nullptr, *abz = nullptr;
+    float4* base = nullptr;
+    float *snp = nullptr, *snq = nullptr;  // halo'd p/q restored from a snapshot
+    float* snaps = nullptr;                // nsnap slots of 4 interior volumes
+    int nsnap = 0;
+    float *grad_vp = nullptr, *grad_rho = nullptr;
+    int64_t src_index = -1;
+    std::vector<float> wavelet;
+    int nrec = 0;
+    int64_t* rec = nullptr;
+    float* traces = nullptr;  // nt*nrec device
+    float* resid = nullptr;   // nt*nrec device
+    float* srctr = nullptr;   // nt device: adjoint p+q at the source
+    bool model_set = false, forward_done = false;
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<int, size_t>> ev_marks;  // (kind, index of start event)
+    double kind_ms[3] = {0, 0, 0};
+    int64_t kind_n[3] = {0, 0, 0};
+    bool sponge_active = false;
+    bool vti = false;
+    int64_t launches = 0;
+    int64_t ninterior = 0;
+
+    int alloc(void** p, size_t bytes)
+    {
+        *p = nullptr;
+        if (bytes == 0) return TTI_OK;
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            return TTI_ENOMEM;
+        }
+        allocs.push_back(*p);
+        return TTI_OK;
+    }
+    int64_t nvol() const { return (int64_t)L.ldimx * L.ldimy * L.ldimz; }
+    dim3 dense_grid() const { return dim3((L.nx() + 127) / 128, L.ny(), L.nz()); }
+};
+
+namespace {
+
+int sim_zero(tti_sim* s, float* p, int64_t n)
+{
+    if (cudaMemsetAsync(p, 0, n * sizeof(float), s->stream) != cudaSuccess) return cuda_rc(cudaGetLastError());
+    return TTI_OK;
+}
+
+// Sponge profile: damping factor G(k) = exp(-(0.3*(W-k)/W)^2) on the k-th cell
+// from an absorbing face (k < W), 1 elsewhere; A = B = G.  The reference
+// ships only all-ones profiles (simulator2SetUp.cu:334-356); its sponge
+// arithmetic (min over axes, A*f + B*dt*rhs) is kept as is.
+std::vector<float2> sponge_axis(int n, int ldim, int width, bool absorb_low)
+{
+    std::vector<float2> ab(ldim, make_float2(1.0f, 1.0f));
+    for (int k = 0; k < width && k < n; ++k) {
+        float g = std::exp(-std::pow(0.3 * (width - k) / (double)width, 2.0));
+        if (absorb_low) ab[kRadius + k] = make_float2(g, g);
+        ab[kRadius + n - 1 - k] = make_float2(fminf(g, ab[kRadius + n - 1 - k].x), fminf(g, ab[kRadius + n - 1 - k].y));
+    }
+    return ab;
+}
+
+int forward_per_kernel_step(tti_sim* s, int n, cudaStream_t st)
+{
+    const Layout& L = s->L;
+    int rc;
+    rc = tti_launch_kernel_loop2(s->f1, s->f2, s->f3, s->f4, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg, L.iyend,
+                                 L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby, (const float*)s->abz,
+                                 s->cfg.dt, st);
+    if (rc) return rc;
+    s->launches++;
+    if (s->cfg.free_surface) {
+        if ((rc = tti_launch_kernel_loop4(s->f1, s->f2, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
+        s->launches++;
+    }
+    float invdx = 1.0 / s->cfg.dx, invdy = 1.0 / s->cfg.dy, invdz = 1.0 / s->cfg.dz;
+    if ((rc = tti_launch_fwd_kernel2_drv(s->f1, s->f2, s->mv[0], s->d[0], s->d[1], s->d[2], s->d[3], s->d[4],
+                                         s->d[5], L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg, L.izend, invdx, invdy,
+                                         invdz, L.ldimx, L.ldimy, 8, st)))
+        return rc;
+    s->launches++;
+    if (s->cfg.free_surface) {
+        if ((rc = tti_launch_kernel_loop4_derivatives(s->d[0], s->d[1], s->d[2], s->d[3], s->d[4], s->d[5], L.ldimx,
+                                                      L.ldimy, L.izbeg, st)))
+            return rc;
+        s->launches++;
+    }
+    // argument order of launch_update_rho_fwd_main_loop_2_1: dx, dx2, dy, dy2, dz, dz2
+    if ((rc = tti_launch_update_rho_fwd_main_loop_2_1(
+             s->f3, s->f4, s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5], s->f1, s->f2, s->mv[0], s->mv[1],
+             s->mv[2], s->mv[3], s->mv[4], s->mv[5], s->mv[6], s->mv[7], nullptr, nullptr, nullptr, nullptr, nullptr,
+             nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, L.ixbeg, L.ixend, L.iybeg, L.iyend,
+             L.izbeg, L.izend, L.ldimx, L.ldimy, s->cfg.dt, s->cfg.dx, s->cfg.dy, s->cfg.dz, 0, 8, 0, 0, 0, st)))
+        return rc;
+    s->launches++;
+    if (s->src_index >= 0) {
+        k_add_source<<<1, 1, 0, st>>>(s->f3, s->f4, s->src_index, s->wavelet[n] * s->cfg.dt);
+        s->launches++;
+    }
+    return launch_status();
+}
+
+int adjoint_per_kernel_step(tti_sim* s, cudaStream_t st)
+{
+    const Layout& L = s->L;
+    const tti_sim_config& c = s->cfg;
+    int rc = launch_base(s->f1, s->f2, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->base, L.ixbeg, L.ixend, L.iybeg,
+                         L.iyend, L.izbeg, L.izend, L.ldimx, L.ldimy, st);
+    if (rc) return rc;
+    rc = launch_adj_drv_with_base(s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5], s->rhs3, s->rhs4, s->base,
+                                  s->mv[0], s->mv[5], s->mv[6], s->mv[7], L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg,
+                                  L.izend, L.ldimx, L.ldimy, (float)(1.0 / (4 * c.dx * c.dy)),
+                                  (float)(1.0 / (4 * c.dy * c.dz)), (float)(1.0 / (4 * c.dx * c.dz)),
+                                  (float)(1.0 / c.dx), (float)(1.0 / c.dy), (float)(1.0 / c.dz), st);
+    if (rc) return rc;
+    s->launches += 2;
+    if (c.free_surface) {
+        if ((rc = tti_launch_kernel_loop4_derivatives(s->d[0], s->d[1], s->d[2], s->d[3], s->d[4], s->d[5], L.ldimx,
+                                                      L.ldimy, L.izbeg, st)))
+            return rc;
+        s->launches++;
+    }
+    if ((rc = tti_launch_update_adj_kernel_main_3(s->f3, s->f4, s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5],
+                                                  s->rhs3, s->rhs4, (const float*)s->abx, (const float*)s->aby,
+                                                  (const float*)s->abz, L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg,
+                                                  L.izend, L.ldimx, L.ldimy, c.dt, c.dx, c.dy, c.dz, 0, 0, 0, 8,
+                                                  s->sponge_active ? 1 : 0, st)))
+        return rc;
+    s->launches++;
+    if ((rc = tti_launch_kernel_loop2(s->f1, s->f2, s->f3, s->f4, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg,
+                                      L.iyend, L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby,
+                                      (const float*)s->abz, c.dt, st)))
+        return rc;
+    s->launches++;
+    if (c.free_surface) {
+        if ((rc = tti_launch_kernel_loop4(s->f1, s->f2, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
+        s->launches++;
+    }
+    return TTI_OK;
+}
+
+// Imaging at a snapshot step (reference order, simulator2SetUp.cu:753-781):
+// Vp image, forward derivatives of the stored p/q, derivative mirror,
+// density gradient with the current adjoint p/q.
+int image_per_kernel(tti_sim* s, const float* slot, cudaStream_t st)
+{
+    const Layout& L = s->L;
+    const tti_sim_config& c = s->cfg;
+    int64_t n = s->ninterior;
+    int rc = tti_launch_update_Vp_gradient(slot, slot + n, s->grad_vp, s->f3, s->f4, L.ixbeg, L.ixend, L.iybeg,
+                                           L.iyend, L.izbeg, L.izend, L.nx(), L.ny(), L.ldimx, L.ldimy, st);
+    if (rc) return rc;
+    k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(s->snp, const_cast<float*>(slot + 2 * n), L);
+    k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(s->snq, const_cast<float*>(slot + 3 * n), L);
+    s->launches += 3;
+    if (c.free_surface) {
+        if ((rc = tti_launch_kernel_loop4(s->snp, s->snq, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
+        s->launches++;
+    }
+    if ((rc = tti_launch_fwd_kernel2_drv(s->snp, s->snq, s->mv[0], s->d[0], s->d[1], s->d[2], s->d[3], s->d[4],
+                                         s->d[5], L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg, L.izend,
+                                         (float)(1.0 / c.dx), (float)(1.0 / c.dy), (float)(1.0 / c.dz), L.ldimx,
+                                         L.ldimy, 8, st)))
+        return rc;
+    s->launches++;
+    if (c.free_surface) {
+        if ((rc = tti_launch_kernel_loop4_derivatives(s->d[0], s->d[1], s->d[2], s->d[3], s->d[4], s->d[5], L.ldimx,
+                                                      L.ldimy, L.izbeg, st)))
+            return rc;
+        s->launches++;
+    }
+    if ((rc = launch_base(s->f1, s->f2, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->base, L.ixbeg, L.ixend, L.iybeg,
+                          L.iyend, L.izbeg, L.izend, L.ldimx, L.ldimy, st)))
+        return rc;
+    if ((rc = launch_rho_gradient_with_base(s->grad_rho, s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5],
+                                            s->base, s->mv[0], s->mv[5], s->mv[6], s->mv[7], L.ixbeg, L.ixend,
+                                            L.iybeg, L.iyend, L.izbeg, L.izend, L.ldimx, L.ldimy, L.nx(), L.ny(), c.dx,
+                                            c.dy, c.dz, st)))
+        return rc;
+    s->launches += 2;
+    return launch_status();
+}
+
+void swap_pq(tti_sim* s)
+{
+    float* t = s->f1;
+    s->f1 = s->g1;
+    s->g1 = t;
+    t = s->f2;
+    s->f2 = s->g2;
+    s->g2 = t;
+}
+
+// Optional per-launch timing of the step kernels (CUDA events on the
+// simulator's stream): kind 0 = forward step, 1 = adjoint step, 2 = imaging.
+cudaEvent_t next_event(tti_sim* s)
+{
+    if (s->ev_used == s->ev_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        s->ev_pool.push_back(e);
+    }
+    return s->ev_pool[s->ev_used++];
+}
+void mark_begin(tti_sim* s, int kind, cudaStream_t st)
+{
+    if (!s->profiling) return;
+    size_t k = s->ev_used;
+    cudaEvent_t e = next_event(s);
+    if (!e) return;
+    cudaEventRecord(e, st);
+    s->ev_marks.push_back({kind, k});
+}
+void mark_end(tti_sim* s, cudaStream_t st)
+{
+    if (!s->profiling || s->ev_marks.empty()) return;
+    cudaEvent_t e = next_event(s);
+    if (e) cudaEventRecord(e, st);
+}
+// After a stream sync: fold the recorded pairs into the per-kind totals.
+void collect_marks(tti_sim* s)
+{
+    for (auto& m : s->ev_marks) {
+        if (m.second + 1 >= s->ev_used) continue;
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, s->ev_pool[m.second], s->ev_pool[m.second + 1]) == cudaSuccess) {
+            s->kind_ms[m.first] += ms;
+            s->kind_n[m.first] += 1;
+        }
+    }
+    cudaGetLastError();
+    s->ev_marks.clear();
+    s->ev_used = 0;
+}
+
+Model model_of(tti_sim* s) { return Model{s->mv[0], s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->mv[5], s->mv[6], s->mv[7]}; }
+
+} // namespace
+
+extern "C" {
+
+int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
+{
+    if (!cfg || !out) return TTI_EINVAL;
+    *out = nullptr;
+    const tti_sim_config& c = *cfg;
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1 || c.nt < 1 || c.xcorr_step < 1 || !(c.dx > 0) || !(c.dy > 0) ||
+        !(c.dz > 0) || !(c.dt > 0) || c.sponge_width < 0 || (c.nz <= kRadius && c.free_surface))
+        return TTI_EINVAL;
+    tti_sim* s = new (std::nothrow) tti_sim();
+    if (!s) return TTI_ENOMEM;
+    s->cfg = c;
+    Layout& L = s->L;
+    L.ldimx = 32 * ((c.nx + 2 * kRadius - 1) / 32 + 1);
+    L.ldimy = c.ny + 2 * kRadius;
+    L.ldimz = c.nz + 2 * kRadius;
+    L.ixbeg = L.iybeg = L.izbeg = kRadius;
+    L.ixend = kRadius + c.nx - 1;
+    L.iyend = kRadius + c.ny - 1;
+    L.izend = kRadius + c.nz - 1;
+    s->ninterior = (int64_t)c.nx * c.ny * c.nz;
+    int rc = TTI_OK;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return TTI_ELAUNCH;
+    }
+    size_t vb = (size_t)s->nvol() * sizeof(float);
+    float** vols[] = {&s->f1, &s->f2, &s->f3, &s->f4, &s->g1, &s->g2, &s->rhs3, &s->rhs4, &s->snp, &s->snq,
+                      &s->d[0], &s->d[1], &s->d[2], &s->d[3], &s->d[4], &s->d[5]};
+    for (float** v : vols)
+        if (!rc) rc = s->alloc((void**)v, vb);
+    for (int k = 0; k < 8 && !rc; ++k) rc = s->alloc((void**)&s->mv[k], vb);
+    if (!rc) rc = s->alloc((void**)&s->base, (size_t)s->nvol() * sizeof(float4));
+    if (!rc) rc = s->alloc((void**)&s->grad_vp, s->ninterior * sizeof(float));
+    if (!rc) rc = s->alloc((void**)&s->grad_rho, s->ninterior * sizeof(float));
+    if (!rc) rc = s->alloc((void**)&s->srctr, (size_t)c.nt * sizeof(float));
+    if (!rc) rc = s->alloc((void**)&s->abx, L.ldimx * sizeof(float2));
+    if (!rc) rc = s->alloc((void**)&s->aby, L.ldimy * sizeof(float2));
+    if (!rc) rc = s->alloc((void**)&s->abz, L.ldimz * sizeof(float2));
+    if (!rc && c.save_snapshots) {
+        s->nsnap = (c.nt - 1) / c.xcorr_step + 1;
+        rc = s->alloc((void**)&s->snaps, (size_t)s->nsnap * 4 * s->ninterior * sizeof(float));
+    }
+    if (!rc) {
+        for (float** v : vols) rc = rc ? rc : sim_zero(s, *v, s->nvol());
+        if (!rc) rc = sim_zero(s, s->grad_vp, s->ninterior);
+        if (!rc) rc = sim_zero(s, s->grad_rho, s->ninterior);
+    }
+    if (!rc) {
+        auto ax = sponge_axis(c.nx, L.ldimx, c.sponge_width, true);
+        auto ay = sponge_axis(c.ny, L.ldimy, c.sponge_width, true);
+        auto az = sponge_axis(c.nz, L.ldimz, c.sponge_width, !c.free_surface);
+        s->sponge_active = c.sponge_width > 0;
+        if (cudaMemcpy(s->abx, ax.data(), ax.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(s->aby, ay.data(), ay.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(s->abz, az.data(), az.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = cuda_rc(cudaGetLastError());
+    }
+    if (!rc) rc = cuda_rc(cudaStreamSynchronize(s->stream));
+    if (rc) {
+        tti_sim_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return TTI_OK;
+}
+
+int tti_sim_destroy(tti_sim* s)
+{
+    if (!s) return TTI_EINVAL;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    cudaGetLastError();
+    delete s;
+    return TTI_OK;
+}
+
+int tti_sim_set_model(tti_sim* s, const float* vp, const float* eps, const float* delta, const float* vs,
+                      const float* theta, const float* phi, const float* rho)
+{
+    if (!s || !vp) return TTI_EINVAL;
+    const int64_t n = s->ninterior;
+    const Layout& L = s->L;
+    cudaStream_t st = s->stream;
+    // Six host parameter arrays (plus rho) uploaded as interior arrays, then
+    // edge-extended into halo'd volumes and turned into model1..7.
+    std::vector<float> defaults[7];
+    const float* src[7] = {vp, eps, delta, vs, theta, phi, rho};
+    const float dflt[7] = {0, 0, 0, 0, 0, 0, 1};
+    for (int k = 1; k < 7; ++k)
+        if (!src[k]) {
+            defaults[k].assign(n, dflt[k]);
+            src[k] = defaults[k].data();
+        }
+    bool vti = true;
+    for (int64_t i = 0; i < n && vti; ++i) vti = (src[4][i] == 0.0f);
+    s->vti = vti;
+    float* dense = nullptr;
+    float* par[7] = {};
+    int rc = TTI_OK;
+    if (cudaMalloc(&dense, n * sizeof(float)) != cudaSuccess) return cuda_rc(cudaGetLastError());
+    for (int k = 0; k < 7 && !rc; ++k) {
+        if (cudaMalloc(&par[k], s->nvol() * sizeof(float)) != cudaSuccess) {
+            rc = cuda_rc(cudaGetLastError());
+            break;
+        }
+        if (cudaMemcpyAsync(dense, src[k], n * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+            rc = cuda_rc(cudaGetLastError());
+            break;
+        }
+        k_scatter_extend<<<dim3((L.ldimx + 127) / 128, L.ldimy, L.ldimz), 128, 0, st>>>(par[k], dense, L);
+        rc = launch_status();
+        if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
+    }
+    if (!rc)
+        rc = tti_launch_init_cijs(par[0], par[1], par[2], par[3], par[4], par[5], s->mv[1], s->mv[2], s->mv[3],
+                                  s->mv[4], s->mv[5], s->mv[6], s->mv[7], s->nvol(), st);
+    if (!rc) {
+        // buoyancy irho = 1/rho (the reference leaves Model11 unset, kernel_type2.cu:136-141)
+        std::vector<float> irho(n);
+        for (int64_t i = 0; i < n; ++i) irho[i] = 1.0f / src[6][i];
+        if (cudaMemcpyAsync(dense, irho.data(), n * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess)
+            rc = cuda_rc(cudaGetLastError());
+        if (!rc) {
+            k_scatter_extend<<<dim3((L.ldimx + 127) / 128, L.ldimy, L.ldimz), 128, 0, st>>>(s->mv[0], dense, L);
+            rc = launch_status();
+        }
+        if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
+    }
+    cudaStreamSynchronize(st);
+    cudaFree(dense);
+    for (float* p : par) cudaFree(p);
+    if (!rc) s->model_set = true;
+    return rc;
+}
+
+int tti_sim_set_source(tti_sim* s, int ix, int iy, int iz, const float* w, int nt)
+{
+    if (!s || !w || nt < s->cfg.nt) return TTI_EINVAL;
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= s->cfg.nx || iy >= s->cfg.ny || iz >= s->cfg.nz) return TTI_EINVAL;
+    s->src_index = s->L.idx(ix + kRadius, iy + kRadius, iz + kRadius);
+    s->wavelet.assign(w, w + s->cfg.nt);
+    return TTI_OK;
+}
+
+int tti_sim_set_receivers(tti_sim* s, int nrec, const int* ixyz)
+{
+    if (!s || nrec < 0 || (nrec > 0 && !ixyz)) return TTI_EINVAL;
+    std::vector<int64_t> idx(nrec);
+    for (int r = 0; r < nrec; ++r) {
+        int ix = ixyz[3 * r], iy = ixyz[3 * r + 1], iz = ixyz[3 * r + 2];
+        if (ix < 0 || iy < 0 || iz < 0 || ix >= s->cfg.nx || iy >= s->cfg.ny || iz >= s->cfg.nz) return TTI_EINVAL;
+        idx[r] = s->L.idx(ix + kRadius, iy + kRadius, iz + kRadius);
+    }
+    std::vector<int64_t> sorted(idx);
+    std::sort(sorted.begin(), sorted.end());
+    for (int r = 1; r < nrec; ++r)
+        if (sorted[r] == sorted[r - 1]) return TTI_EINVAL;
+    for (void** p : {(void**)&s->rec, (void**)&s->traces, (void**)&s->resid}) {
+        if (*p) {
+            cudaFree(*p);
+            for (auto& a : s->allocs)
+                if (a == *p) a = nullptr;
+            *p = nullptr;
+        }
+    }
+    s->nrec = nrec;
+    if (nrec == 0) return TTI_OK;
+    int rc = s->alloc((void**)&s->rec, nrec * sizeof(int64_t));
+    if (!rc) rc = s->alloc((void**)&s->traces, (size_t)nrec * s->cfg.nt * sizeof(float));
+    if (!rc) rc = s->alloc((void**)&s->resid, (size_t)nrec * s->cfg.nt * sizeof(float));
+    if (!rc && cudaMemcpy(s->rec, idx.data(), nrec * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = cuda_rc(cudaGetLastError());
+    return rc;
+}
+
+int tti_sim_forward(tti_sim* s, float* traces, int traces_on_device)
+{
+    if (!s || !s->model_set) return s ? TTI_ESTATE : TTI_EINVAL;
+    const tti_sim_config& c = s->cfg;
+    const Layout& L = s->L;
+    cudaStream_t st = s->stream;
+    s->launches = 0;
+    int rc = TTI_OK;
+    for (float* v : {s->f1, s->f2, s->f3, s->f4, s->g1, s->g2})
+        if (!rc) rc = sim_zero(s, v, s->nvol());
+    if (rc) return rc;
+    const bool fused = c.fused != 0;
+    if (fused) {
+        // Step-0 p update of the reference step (loop2 + free surface); the
+        // fused kernel of step n then ends with the p update of step n+1.
+        rc = tti_launch_kernel_loop2(s->f1, s->f2, s->f3, s->f4, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg,
+                                     L.iyend, L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby,
+                                     (const float*)s->abz, c.dt, st);
+        s->launches++;
+        if (!rc && c.free_surface) {
+            rc = tti_launch_kernel_loop4(s->f1, s->f2, L.ldimx, L.ldimy, L.izbeg, st);
+            s->launches++;
+        }
+        if (rc) return rc;
+    }
+    for (int n = 0; n < c.nt; ++n) {
+        const bool snap = c.save_snapshots && (n % c.xcorr_step == 0);
+        float* slot = snap ? s->snaps + (size_t)(n / c.xcorr_step) * 4 * s->ninterior : nullptr;
+        if (!fused) {
+            if ((rc = forward_per_kernel_step(s, n, st))) return rc;
+            if (snap) {
+                k_snapshot_save<<<s->dense_grid(), 128, 0, st>>>(slot, s->f3, s->f4, s->f1, s->f2, L);
+                s->launches++;
+            }
+            if (s->nrec) {
+                k_receivers<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->traces + (size_t)n * s->nrec, s->f1, s->f2,
+                                                                  s->rec, s->nrec);
+                s->launches++;
+            }
+        } else {
+            if (s->nrec) {
+                k_receivers<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->traces + (size_t)n * s->nrec, s->f1, s->f2,
+                                                                  s->rec, s->nrec);
+                s->launches++;
+            }
+            FwdStepArgs a{};
+            a.pin = s->f1;
+            a.qin = s->f2;
+            a.pout = s->g1;
+            a.qout = s->g2;
+            a.f3 = s->f3;
+            a.f4 = s->f4;
+            a.m = model_of(s);
+            a.abx = s->abx;
+            a.aby = s->aby;
+            a.abz = s->abz;
+            a.src_index = s->src_index;
+            a.src_term = s->src_index >= 0 ? s->wavelet[n] * c.dt : 0.0f;
+            a.snap = slot;
+            a.free_surface = c.free_surface;
+            a.vti = s->vti ? 1 : 0;
+            a.dt = c.dt;
+            a.dx = c.dx;
+            a.dy = c.dy;
+            a.dz = c.dz;
+            mark_begin(s, 0, st);
+            rc = launch_fused_forward(L, a, st);
+            mark_end(s, st);
+            if (rc) return rc;
+            s->launches++;
+            swap_pq(s);
+        }
+        if ((rc = launch_status())) return rc;
+    }
+    if (traces && s->nrec) {
+        size_t bytes = (size_t)s->nrec * c.nt * sizeof(float);
+        cudaError_t e = cudaMemcpyAsync(traces, s->traces, bytes,
+                                        traces_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return cuda_rc(e);
+    }
+    rc = cuda_rc(cudaStreamSynchronize(st));
+    if (!rc && fused) rc = fused_wait_status(st);
+    collect_marks(s);
+    if (!rc) s->forward_done = true;
+    return rc;
+}
+
+static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device, bool observed);
+
+int tti_sim_adjoint(tti_sim* s, const float* residual, int residual_on_device)
+{
+    return sim_adjoint(s, residual, residual_on_device, false);
+}
+
+int tti_sim_adjoint_observed(tti_sim* s, const float* observed, int observed_on_device)
+{
+    if (!s || !observed) return TTI_EINVAL;
+    return sim_adjoint(s, observed, observed_on_device, true);
+}
+
+static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device, bool observed)
+{
+    if (!s) return TTI_EINVAL;
+    if (!s->model_set || !s->forward_done || !s->cfg.save_snapshots) return TTI_ESTATE;
+    const tti_sim_config& c = s->cfg;
+    const Layout& L = s->L;
+    cudaStream_t st = s->stream;
+    s->launches = 0;
+    int rc = TTI_OK;
+    for (float* v : {s->f1, s->f2, s->f3, s->f4, s->g1, s->g2})
+        if (!rc) rc = sim_zero(s, v, s->nvol());
+    if (!rc) rc = sim_zero(s, s->grad_vp, s->ninterior);
+    if (!rc) rc = sim_zero(s, s->grad_rho, s->ninterior);
+    if (rc) return rc;
+    if (s->nrec && residual) {
+        size_t bytes = (size_t)s->nrec * c.nt * sizeof(float);
+        cudaError_t e = cudaMemcpyAsync(s->resid, residual, bytes,
+                                        residual_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_rc(e);
+    } else if (s->nrec) {
+        if ((rc = sim_zero(s, s->resid, (int64_t)s->nrec * c.nt))) return rc;
+    }
+    const bool fused = c.fused != 0;
+    for (int n = c.nt - 1; n >= 0; --n) {
+        if (s->src_index >= 0) {
+            k_source_trace<<<1, 1, 0, st>>>(s->srctr + n, s->f1, s->f2, s->src_index);
+            s->launches++;
+        }
+        if (s->nrec) {
+            const float* obs = observed ? s->resid + (size_t)n * s->nrec : nullptr;
+            const float* res = observed ? s->traces + (size_t)n * s->nrec : s->resid + (size_t)n * s->nrec;
+            k_inject_residual<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->f3, s->f4, s->rec, res, obs, s->nrec);
+            s->launches++;
+        }
+        if (!fused) {
+            if ((rc = adjoint_per_kernel_step(s, st))) return rc;
+        } else {
+            AdjStepArgs a{};
+            a.pin = s->f1;
+            a.qin = s->f2;
+            a.pout = s->g1;
+            a.qout = s->g2;
+            a.f3 = s->f3;
+            a.f4 = s->f4;
+            a.m = model_of(s);
+            a.abx = s->abx;
+            a.aby = s->aby;
+            a.abz = s->abz;
+            a.sponge_active = s->sponge_active ? 1 : 0;
+            a.free_surface = c.free_surface;
+            a.vti = s->vti ? 1 : 0;
+            a.dt = c.dt;
+            a.dx = c.dx;
+            a.dy = c.dy;
+            a.dz = c.dz;
+            mark_begin(s, 1, st);
+            rc = launch_fused_adjoint(L, a, st);
+            mark_end(s, st);
+            if (rc) return rc;
+            s->launches++;
+            swap_pq(s);
+        }
+        if (n % c.xcorr_step == 0) {
+            const float* slot = s->snaps + (size_t)(n / c.xcorr_step) * 4 * s->ninterior;
+            mark_begin(s, 2, st);
+            rc = image_per_kernel(s, slot, st);
+            mark_end(s, st);
+            if (rc) return rc;
+        }
+        if ((rc = launch_status())) return rc;
+    }
+    k_finalize_dense<<<s->dense_grid(), 128, 0, st>>>(s->grad_vp, s->mv[3], L, c.dt * c.xcorr_step);
+    s->launches++;
+    rc = cuda_rc(cudaStreamSynchronize(st));
+    if (!rc && fused) rc = fused_wait_status(st);
+    collect_marks(s);
+    return rc;
+}
+
+int tti_sim_get_image(tti_sim* s, float* grad_vp, float* grad_rho, int on_device)
+{
+    if (!s) return TTI_EINVAL;
+    size_t bytes = s->ninterior * sizeof(float);
+    cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (grad_vp && cudaMemcpyAsync(grad_vp, s->grad_vp, bytes, k, s->stream) != cudaSuccess)
+        return cuda_rc(cudaGetLastError());
+    if (grad_rho && cudaMemcpyAsync(grad_rho, s->grad_rho, bytes, k, s->stream) != cudaSuccess)
+        return cuda_rc(cudaGetLastError());
+    return cuda_rc(cudaStreamSynchronize(s->stream));
+}
+
+int tti_sim_set_profiling(tti_sim* s, int enable)
+{
+    if (!s) return TTI_EINVAL;
+    s->profiling = enable != 0;
+    for (int k = 0; k < 3; ++k) {
+        s->kind_ms[k] = 0;
+        s->kind_n[k] = 0;
+    }
+    return TTI_OK;
+}
+
+int tti_sim_kernel_times(tti_sim* s, double* ms, int64_t* launches)
+{
+    if (!s || !ms || !launches) return TTI_EINVAL;
+    for (int k = 0; k < 3; ++k) {
+        ms[k] = s->kind_ms[k];
+        launches[k] = s->kind_n[k];
+    }
+    return TTI_OK;
+}
+
+int tti_sim_source_gradient(tti_sim* s, float* host_out)
+{
+    if (!s || !host_out) return TTI_EINVAL;
+    if (s->src_index < 0) return TTI_ESTATE;
+    std::vector<float> tmp(s->cfg.nt);
+    if (cudaMemcpyAsync(tmp.data(), s->srctr, s->cfg.nt * sizeof(float), cudaMemcpyDeviceToHost, s->stream) !=
+        cudaSuccess)
+        return cuda_rc(cudaGetLastError());
+    int rc = cuda_rc(cudaStreamSynchronize(s->stream));
+    if (rc) return rc;
+    for (int n = 0; n < s->cfg.nt; ++n) host_out[n] = tmp[n] * s->cfg.dt;
+    return TTI_OK;
+}
+
+int tti_sim_volume(tti_sim* s, int which, float** dev_ptr)
+{
+    if (!s || !dev_ptr || which < 0 || which > 11) return TTI_EINVAL;
+    float* v[12] = {s->f1, s->f2, s->f3, s->f4, s->mv[0], s->mv[1], s->mv[2], s->mv[3],
+                    s->mv[4], s->mv[5], s->mv[6], s->mv[7]};
+    *dev_ptr = v[which];
+    return TTI_OK;
+}
+
+int tti_sim_read_volume(tti_sim* s, int which, float* host_dst)
+{
+    float* src = nullptr;
+    int rc = tti_sim_volume(s, which, &src);
+    if (rc) return rc;
+    if (!host_dst) return TTI_EINVAL;
+    if (cudaMemcpyAsync(host_dst, src, s->nvol() * sizeof(float), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+        return cuda_rc(cudaGetLastError());
+    return cuda_rc(cudaStreamSynchronize(s->stream));
+}
+
+int tti_sim_layout(tti_sim* s, int* ldimx, int* ldimy, int* ldimz)
+{
+    if (!s || !ldimx || !ldimy || !ldimz) return TTI_EINVAL;
+    *ldimx = s->L.ldimx;
+    *ldimy = s->L.ldimy;
+    *ldimz = s->L.ldimz;
+    return TTI_OK;
+}
+
+int64_t tti_sim_launch_count(tti_sim* s) { return s ? s->launches : -1; }
+
+tti_stream_t tti_sim_stream(tti_sim* s) { return s ? (tti_stream_t)s->stream : nullptr; }
+
+} // extern "C"

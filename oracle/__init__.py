@@ -1,0 +1,258 @@
+"""CPU oracle for the TTI/VTI RTM hot path -- TEST INFRASTRUCTURE ONLY.
+
+Python bindings (ctypes + numpy) over ``liboracle_tti.so``, the plain-C
+restatement of the reference kernels in ``tti_oracle.c``.  Only the tests,
+the smoke check and the CPU-baseline leg of ``bench.py`` may import this
+package; the product library never does.
+
+``Layout`` describes the reference volume layout (x fastest, radius-4 halo
+on every axis, ``ldimx`` padded to 32 floats: infrastructure/axis.cpp:78-99,
+utils/volume_index.h:20-23).  Volumes are numpy arrays of shape
+``(ldimz, ldimy, ldimx)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_tti.so")
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libref_tti.so")
+RADIUS = 4
+
+
+def pad32(n: int) -> int:
+    return 32 * ((n - 1) // 32 + 1)
+
+
+@dataclass(frozen=True)
+class Layout:
+    """Interior grid (nx, ny, nz) with the reference's halo/padding layout."""
+
+    nx: int
+    ny: int
+    nz: int
+
+    @property
+    def ldimx(self) -> int:
+        return pad32(self.nx + 2 * RADIUS)
+
+    @property
+    def ldimy(self) -> int:
+        return self.ny + 2 * RADIUS
+
+    @property
+    def ldimz(self) -> int:
+        return self.nz + 2 * RADIUS
+
+    @property
+    def shape(self):
+        return (self.ldimz, self.ldimy, self.ldimx)
+
+    @property
+    def nvol(self) -> int:
+        return self.ldimx * self.ldimy * self.ldimz
+
+    @property
+    def ranges(self):
+        """(ixbeg, ixend, iybeg, iyend, izbeg, izend), inclusive, halo excluded."""
+        r = RADIUS
+        return (r, r + self.nx - 1, r, r + self.ny - 1, r, r + self.nz - 1)
+
+    @property
+    def interior(self):
+        r = RADIUS
+        return (slice(r, r + self.nz), slice(r, r + self.ny), slice(r, r + self.nx))
+
+    def zeros(self, dtype=np.float32):
+        return np.zeros(self.shape, dtype=dtype)
+
+    def index(self, ix: int, iy: int, iz: int) -> int:
+        """Flat index of an interior cell given 0-based interior coordinates."""
+        r = RADIUS
+        return ((iz + r) * self.ldimy + (iy + r)) * self.ldimx + (ix + r)
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C-contiguous"
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class OrcGrid(C.Structure):
+    _fields_ = [
+        ("ldimx", C.c_int), ("ldimy", C.c_int), ("ldimz", C.c_int),
+        ("ixbeg", C.c_int), ("ixend", C.c_int), ("iybeg", C.c_int), ("iyend", C.c_int),
+        ("izbeg", C.c_int), ("izend", C.c_int),
+        ("free_surface", C.c_int), ("sponge_active", C.c_int),
+        ("dt", C.c_float), ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+    ]
+
+
+V, I, F, D, L = C.c_void_p, C.c_int, C.c_float, C.c_double, C.c_int64
+_SIGS = {
+    "orc_coefficients": [V, V, V],
+    "orc_loop2": [V, V, V, V, I, I, I, I, I, I, I, I, V, V, V, F],
+    "orc_loop4": [V, V, I, I, I],
+    "orc_fwd_drv": [V] * 9 + [I] * 6 + [F] * 3 + [I, I],
+    "orc_loop4_derivatives": [V] * 6 + [I, I, I],
+    "orc_fwd_update": [V] * 18 + [I] * 8 + [F, D, D, D],
+    "orc_adj_drv": [V] * 18 + [I] * 6 + [F] * 3 + [I, I] + [F] * 3,
+    "orc_adj_update": [V] * 13 + [I] * 8 + [F, D, D, D, I],
+    "orc_update_vp_gradient": [V] * 5 + [I] * 10,
+    "orc_finalize_vp_gradient": [V, V] + [I] * 10 + [F],
+    "orc_rho_gradient": [V] * 17 + [I] * 10 + [D, D, D],
+    "orc_init_cijs": [V] * 13 + [L],
+    "orc_pressure": [V, V, V, L],
+    "orc_fwd_step": [C.POINTER(OrcGrid)] + [V] * 21 + [L, F, I, V, V],
+    "orc_adj_step": [C.POINTER(OrcGrid)] + [V] * 23 + [I, V, V],
+    "orc_num_threads": [],
+}
+
+
+class Oracle:
+    """One precision of the C oracle: ``Oracle('f32')`` or ``Oracle('f64')``."""
+
+    def __init__(self, precision: str = "f32"):
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run `make -C oracle`")
+        self.lib = C.CDLL(LIB_PATH)
+        self.precision = precision
+        self.dtype = np.float32 if precision == "f32" else np.float64
+        self.fn = {}
+        for name, sig in _SIGS.items():
+            f = getattr(self.lib, f"{name}_{precision}")
+            f.argtypes = sig
+            f.restype = I if name == "orc_num_threads" else None
+            self.fn[name] = f
+
+    def _chk(self, *arrs):
+        for a in arrs:
+            if a is not None and a.dtype != self.dtype:
+                raise TypeError(f"expected {self.dtype}, got {a.dtype}")
+
+    @staticmethod
+    def coefficients():
+        c1 = np.zeros(5, np.float32)
+        c2 = np.zeros(5, np.float32)
+        cs = np.zeros(4, np.float32)
+        lib = C.CDLL(LIB_PATH)
+        f = lib.orc_coefficients_f32
+        f.argtypes = [V, V, V]
+        f(_p(c1), _p(c2), _p(cs))
+        return c1, c2, cs
+
+    def num_threads(self) -> int:
+        return int(self.fn["orc_num_threads"]())
+
+    # --- per-kernel restatements ------------------------------------------
+    def loop2(self, lay: Layout, f1, f2, f3, f4, abx, aby, abz, dt):
+        self._chk(f1, f2, f3, f4)
+        self.fn["orc_loop2"](_p(f1), _p(f2), _p(f3), _p(f4), lay.ldimx, lay.ldimy, *lay.ranges,
+                             _p(abx), _p(aby), _p(abz), dt)
+
+    def loop4(self, lay: Layout, f1, f2):
+        self._chk(f1, f2)
+        self.fn["orc_loop4"](_p(f1), _p(f2), lay.ldimx, lay.ldimy, RADIUS)
+
+    def fwd_drv(self, lay: Layout, f1, f2, irho, d, invd):
+        """d: dict with keys d1x,d1y,d1z,d2x,d2y,d2z."""
+        self._chk(f1, f2, irho, *d.values())
+        self.fn["orc_fwd_drv"](_p(f1), _p(f2), _p(irho), _p(d["d1x"]), _p(d["d1y"]), _p(d["d1z"]),
+                               _p(d["d2x"]), _p(d["d2y"]), _p(d["d2z"]), *lay.ranges, *invd,
+                               lay.ldimx, lay.ldimy)
+
+    def loop4_derivatives(self, lay: Layout, d):
+        self.fn["orc_loop4_derivatives"](_p(d["d1x"]), _p(d["d1y"]), _p(d["d1z"]), _p(d["d2x"]),
+                                         _p(d["d2y"]), _p(d["d2z"]), lay.ldimx, lay.ldimy, RADIUS)
+
+    def fwd_update(self, lay: Layout, f3, f4, d, f1, f2, m, dt, h):
+        """m: dict irho,m1,m2,m3,m4,rx,ry,rz; h = (dx, dy, dz)."""
+        self._chk(f3, f4, f1, f2)
+        self.fn["orc_fwd_update"](_p(f3), _p(f4), _p(d["d1x"]), _p(d["d2x"]), _p(d["d1y"]),
+                                  _p(d["d2y"]), _p(d["d1z"]), _p(d["d2z"]), _p(f1), _p(f2),
+                                  _p(m["irho"]), _p(m["m1"]), _p(m["m2"]), _p(m["m3"]), _p(m["m4"]),
+                                  _p(m["rx"]), _p(m["ry"]), _p(m["rz"]), *lay.ranges, lay.ldimx,
+                                  lay.ldimy, dt, *h)
+
+    def adj_drv(self, lay: Layout, d, rhs3, rhs4, f1, f2, m, h):
+        dx, dy, dz = h
+        self._chk(rhs3, rhs4, f1, f2)
+        self.fn["orc_adj_drv"](_p(d["d1x"]), _p(d["d2x"]), _p(d["d1y"]), _p(d["d2y"]), _p(d["d1z"]),
+                               _p(d["d2z"]), _p(rhs3), _p(rhs4), _p(f1), _p(f2), _p(m["irho"]),
+                               _p(m["m1"]), _p(m["m2"]), _p(m["m3"]), _p(m["m4"]), _p(m["rx"]),
+                               _p(m["ry"]), _p(m["rz"]), *lay.ranges,
+                               np.float32(1.0 / (4 * dx * dy)), np.float32(1.0 / (4 * dy * dz)),
+                               np.float32(1.0 / (4 * dx * dz)), lay.ldimx, lay.ldimy,
+                               np.float32(1.0 / dx), np.float32(1.0 / dy), np.float32(1.0 / dz))
+
+    def adj_update(self, lay: Layout, f3, f4, d, rhs3, rhs4, abx, aby, abz, dt, h, sponge_active):
+        self._chk(f3, f4, rhs3, rhs4)
+        self.fn["orc_adj_update"](_p(f3), _p(f4), _p(d["d1x"]), _p(d["d2x"]), _p(d["d1y"]),
+                                  _p(d["d2y"]), _p(d["d1z"]), _p(d["d2z"]), _p(rhs3), _p(rhs4),
+                                  _p(abx), _p(aby), _p(abz), *lay.ranges, lay.ldimx, lay.ldimy, dt,
+                                  *h, int(sponge_active))
+
+    def update_vp_gradient(self, lay: Layout, snap3, snap4, grad, adj3, adj4):
+        self.fn["orc_update_vp_gradient"](_p(snap3), _p(snap4), _p(grad), _p(adj3), _p(adj4),
+                                          *lay.ranges, lay.nx, lay.ny, lay.ldimx, lay.ldimy)
+
+    def finalize_vp_gradient(self, lay: Layout, model3, grad, dt_xcorr):
+        self.fn["orc_finalize_vp_gradient"](_p(model3), _p(grad), *lay.ranges, lay.nx, lay.ny,
+                                            lay.ldimx, lay.ldimy, dt_xcorr)
+
+    def rho_gradient(self, lay: Layout, grad, fd, f1, f2, m, h, grad_ldimx=None, grad_ldimy=None):
+        gx = lay.ldimx if grad_ldimx is None else grad_ldimx
+        gy = lay.ldimy if grad_ldimy is None else grad_ldimy
+        self.fn["orc_rho_gradient"](_p(grad), _p(fd["d1x"]), _p(fd["d2x"]), _p(fd["d1y"]),
+                                    _p(fd["d2y"]), _p(fd["d1z"]), _p(fd["d2z"]), _p(f1), _p(f2),
+                                    _p(m["irho"]), _p(m["m1"]), _p(m["m2"]), _p(m["m3"]),
+                                    _p(m["m4"]), _p(m["rx"]), _p(m["ry"]), _p(m["rz"]), *lay.ranges,
+                                    lay.ldimx, lay.ldimy, gx, gy, *h)
+
+    def init_cijs(self, vp, eps, delta, vs, theta, phi):
+        n = vp.size
+        out = [np.zeros(vp.shape, self.dtype) for _ in range(7)]
+        args = [np.ascontiguousarray(a, np.float32) for a in (vp, eps, delta, vs, theta, phi)]
+        self.fn["orc_init_cijs"](*[_p(a) for a in args], *[_p(o) for o in out], n)
+        return out
+
+    # --- step drivers ------------------------------------------------------
+    def grid(self, lay: Layout, dt, h, free_surface=True, sponge_active=False) -> OrcGrid:
+        return OrcGrid(lay.ldimx, lay.ldimy, lay.ldimz, *lay.ranges, int(free_surface),
+                       int(sponge_active), dt, *h)
+
+    def fwd_step(self, g: OrcGrid, st, m, ab, src_index=-1, src_amp=0.0, rec_index=None,
+                 traces=None):
+        d = st["d"]
+        nrec = 0 if rec_index is None else len(rec_index)
+        self.fn["orc_fwd_step"](C.byref(g), _p(st["f1"]), _p(st["f2"]), _p(st["f3"]), _p(st["f4"]),
+                                _p(d["d1x"]), _p(d["d1y"]), _p(d["d1z"]), _p(d["d2x"]), _p(d["d2y"]),
+                                _p(d["d2z"]), _p(m["irho"]), _p(m["m1"]), _p(m["m2"]), _p(m["m3"]),
+                                _p(m["m4"]), _p(m["rx"]), _p(m["ry"]), _p(m["rz"]), _p(ab[0]),
+                                _p(ab[1]), _p(ab[2]), int(src_index), float(src_amp), nrec,
+                                _p(rec_index), _p(traces))
+
+    def adj_step(self, g: OrcGrid, st, m, ab, rec_index=None, residual=None):
+        d = st["d"]
+        nrec = 0 if rec_index is None else len(rec_index)
+        self.fn["orc_adj_step"](C.byref(g), _p(st["f1"]), _p(st["f2"]), _p(st["f3"]), _p(st["f4"]),
+                                _p(d["d1x"]), _p(d["d1y"]), _p(d["d1z"]), _p(d["d2x"]), _p(d["d2y"]),
+                                _p(d["d2z"]), _p(st["rhs3"]), _p(st["rhs4"]), _p(m["irho"]),
+                                _p(m["m1"]), _p(m["m2"]), _p(m["m3"]), _p(m["m4"]), _p(m["rx"]),
+                                _p(m["ry"]), _p(m["rz"]), _p(ab[0]), _p(ab[1]), _p(ab[2]), nrec,
+                                _p(rec_index), _p(residual))
+
+
+DKEYS = ("d1x", "d1y", "d1z", "d2x", "d2y", "d2z")
+MKEYS = ("irho", "m1", "m2", "m3", "m4", "rx", "ry", "rz")
+
+
+def new_state(lay: Layout, dtype=np.float32):
+    st = {k: lay.zeros(dtype) for k in ("f1", "f2", "f3", "f4", "rhs3", "rhs4")}
+    st["d"] = {k: lay.zeros(dtype) for k in DKEYS}
+    return st

@@ -1,0 +1,117 @@
+"""Shared helpers for the tests: seeded inputs in the reference layout and
+comparison metrics."""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import DKEYS, MKEYS, Layout, RADIUS
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    den = np.linalg.norm(b.ravel())
+    num = np.linalg.norm((a - b).ravel())
+    return float(num / den) if den > 0 else float(num)
+
+
+def random_model(lay: Layout, rng, tti=True, halo_safe=True):
+    """Random but physically plausible model volumes over the whole halo'd
+    allocation (the reference kernels read model halos)."""
+    sh = lay.shape
+    vp = rng.uniform(1800.0, 3200.0, sh)
+    eps = rng.uniform(0.0, 0.25, sh)
+    delta = eps * rng.uniform(0.0, 0.6, sh)
+    vs = rng.uniform(0.0, 400.0, sh)
+    theta = rng.uniform(0.0, 0.8, sh) if tti else np.zeros(sh)
+    phi = rng.uniform(0.0, 3.0, sh) if tti else np.zeros(sh)
+    m1 = vp * vp * (1 + 2 * eps)
+    m2 = np.sqrt((vp * vp - vs * vs) * (vp * vp * (1 + 2 * delta) - vs * vs))
+    m = dict(m1=m1, m2=m2, m3=vp * vp, m4=vs * vs, rx=np.sin(theta) * np.cos(phi),
+             ry=np.sin(theta) * np.sin(phi), rz=np.cos(theta),
+             irho=1.0 / rng.uniform(1.0, 2.5, sh))
+    return {k: np.ascontiguousarray(v, np.float32) for k, v in m.items()}
+
+
+def random_field(lay: Layout, rng, scale=1.0, halo=True):
+    a = (scale * rng.standard_normal(lay.shape)).astype(np.float32)
+    if not halo:
+        b = np.zeros_like(a)
+        b[lay.interior] = a[lay.interior]
+        a = b
+    return a
+
+
+def sponge_ab(n_alloc, rng, active=True):
+    ab = np.ones((n_alloc, 2), np.float32)
+    if active:
+        ab[:, 0] = rng.uniform(0.9, 1.0, n_alloc)
+        ab[:, 1] = rng.uniform(0.9, 1.0, n_alloc)
+    return np.ascontiguousarray(ab.reshape(-1))
+
+
+def sponge_profile(n: int, ldim: int, width: int, absorb_low: bool):
+    """The simulator's sponge (A,B) pairs per global index (host logic mirror)."""
+    ab = np.ones((ldim, 2), np.float32)
+    for k in range(min(width, n)):
+        g = np.float32(np.exp(-((0.3 * (width - k) / width) ** 2)))
+        if absorb_low:
+            ab[RADIUS + k] = g
+        ab[RADIUS + n - 1 - k] = np.minimum(ab[RADIUS + n - 1 - k], g)
+    return np.ascontiguousarray(ab.reshape(-1))
+
+
+def sim_models(sim):
+    names = ("irho", "model1", "model2", "model3", "model4", "rx", "ry", "rz")
+    keys = ("irho", "m1", "m2", "m3", "m4", "rx", "ry", "rz")
+    return {k: np.ascontiguousarray(sim.volume(n)) for k, n in zip(keys, names)}
+
+
+def oracle_rtm(o, lay, m, ab, cfg, src, wavelet, rec, residual=None, adjoint=True):
+    """Reference-order RTM with the oracle: forward with snapshots every
+    xcorr_step steps, adjoint driven by residual traces, Vp image and density
+    gradient at snapshot steps (simulator2SetUp.cu:517-782 with nsub = 1)."""
+    from oracle import new_state
+
+    dt = np.float32(cfg.dt)
+    h = (cfg.dx, cfg.dy, cfg.dz)
+    g = o.grid(lay, dt, h, free_surface=cfg.free_surface, sponge_active=cfg.sponge_width > 0)
+    st = new_state(lay, o.dtype)
+    nrec = len(rec)
+    traces = np.zeros((cfg.nt, nrec), o.dtype)
+    snaps = {}
+    I = lay.interior
+    for n in range(cfg.nt):
+        row = np.zeros(nrec, o.dtype)
+        o.fwd_step(g, st, m, ab, src, float(wavelet[n]), rec, row)
+        traces[n] = row
+        if n % cfg.xcorr_step == 0:
+            snaps[n] = [st[k][I].copy() for k in ("f3", "f4", "f1", "f2")]
+    out = {"traces": traces, "f3": st["f3"].copy(), "f4": st["f4"].copy()}
+    if not adjoint:
+        return out
+    res = traces if residual is None else residual.astype(o.dtype)
+    adj = new_state(lay, o.dtype)
+    n_in = lay.nx * lay.ny * lay.nz
+    gvp = np.zeros(n_in, o.dtype)
+    grho = np.zeros(n_in, o.dtype)
+    for n in range(cfg.nt - 1, -1, -1):
+        o.adj_step(g, adj, m, ab, rec, np.ascontiguousarray(res[n]))
+        if n % cfg.xcorr_step == 0:
+            s3, s4, s1, s2 = snaps[n]
+            o.update_vp_gradient(lay, np.ascontiguousarray(s3.ravel()), np.ascontiguousarray(s4.ravel()),
+                                 gvp, adj["f3"], adj["f4"])
+            p, q = lay.zeros(o.dtype), lay.zeros(o.dtype)
+            p[I] = s1
+            q[I] = s2
+            if cfg.free_surface:
+                o.loop4(lay, p, q)
+            d = {k: lay.zeros(o.dtype) for k in DKEYS}
+            o.fwd_drv(lay, p, q, m["irho"], d, tuple(np.float32(1.0 / v) for v in h))
+            if cfg.free_surface:
+                o.loop4_derivatives(lay, d)
+            o.rho_gradient(lay, grho, d, adj["f1"], adj["f2"], m, h, lay.nx, lay.ny)
+    o.finalize_vp_gradient(lay, m["m3"], gvp, np.float32(cfg.dt * cfg.xcorr_step))
+    out["grad_vp"] = gvp.reshape(lay.nz, lay.ny, lay.nx)
+    out["grad_rho"] = grho.reshape(lay.nz, lay.ny, lay.nx)
+    return out

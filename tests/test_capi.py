@@ -1,0 +1,71 @@
+"""The C ABI: the library loads, exports every entry point include/tti_capi.h
+declares, and rejects bad arguments with status codes (no GPU needed: the
+argument checks run before any CUDA call)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import miniappsforhpe_b200 as P
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "tti_capi.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tti_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for must in ("tti_launch_fwd_kernel2_drv", "tti_launch_update_rho_fwd_main_loop_2_1",
+                 "tti_launch_adj_kernel2_drv", "tti_launch_update_adj_kernel_main_3",
+                 "tti_launch_update_rho_gradient_rho", "tti_sim_create", "tti_sim_forward",
+                 "tti_sim_adjoint", "tti_snap_start_write", "tti_snap_start_read"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(P.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_version():
+    assert P.status_string(P.OK) == "ok"
+    assert P.status_string(P.ETIMEOUT) == "timed out"
+    assert re.match(r"\d+\.\d+\.\d+", P.version())
+
+
+def test_unsupported_order_is_rejected():
+    with pytest.raises(P.TTIError) as e:
+        P.launch_fwd_kernel2_drv(1, 1, 1, 1, 1, 1, 1, 1, 1, 4, 35, 4, 35, 4, 35, 0.1, 0.1, 0.1, 64, 40,
+                                 order=16)
+    assert e.value.status == P.EINVAL
+
+
+def test_bad_ranges_are_rejected():
+    with pytest.raises(P.TTIError) as e:  # ldimx leaves no radius-4 halo after ixend
+        P.launch_fwd_kernel2_drv(1, 1, 1, 1, 1, 1, 1, 1, 1, 4, 30, 4, 35, 4, 35, 0.1, 0.1, 0.1, 32, 40)
+    assert e.value.status == P.EINVAL
+    with pytest.raises(P.TTIError) as e:  # null volume
+        P.launch_fwd_kernel2_drv(None, 1, 1, 1, 1, 1, 1, 1, 1, 4, 20, 4, 20, 4, 20, 0.1, 0.1, 0.1, 32, 29)
+    assert e.value.status == P.EINVAL
+
+
+def test_pml_is_rejected():
+    lib = P.lib()
+    args = [C.c_void_p(1)] * 18 + [C.c_void_p(1)] + [None] * 11 + [4, 20, 4, 20, 4, 20, 32, 29,
+                                                                    C.c_float(1e-3), 10.0, 10.0, 10.0,
+                                                                    0, 8, 0, 0, 0, None]
+    assert lib.tti_launch_update_rho_fwd_main_loop_2_1(*args) == P.EINVAL
+
+
+def test_sim_config_is_validated():
+    with pytest.raises(P.TTIError) as e:
+        P.Simulator(P.Config(nx=0, ny=8, nz=8))
+    assert e.value.status == P.EINVAL
+    with pytest.raises(P.TTIError):
+        P.Simulator(P.Config(nx=8, ny=8, nz=8, dt=-1.0))
