@@ -30,6 +30,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -819,6 +820,306 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
 }
 
 // ---------------------------------------------------------------------------
+// Fused imaging at a snapshot step: the reference's update_grad_loop_1
+// (Vp image, kernel_type2_small.cu:42-59), snaps_loop (forward derivatives of
+// the stored p/q, kernel_type2.cu:295-303), kernel_loop4_derivative and
+// update_grad_loop_2 (density gradient, kernel_type2_grad.cu:344-509) in one
+// z-marching pass.  The stored p/q come from the device snapshot store (dense
+// interior volumes, free-surface halo re-derived by mirroring); the adjoint
+// temporaries adj_a = rho*(s1 + ra^2 h1) come from the current adjoint p/q.
+struct ImgParams {
+    const float *f3, *f4, *rz, *irho;
+    const float *snap3, *snap4;  // dense pdot/qdot of this snapshot
+    float *gvp, *grho;           // dense images
+    Layout L;
+    int bz;
+    int fs;
+    int slot;                    // snapshot index in the store
+    float hx, hy, hz;
+    int* err;
+};
+
+constexpr int IMG_NSTAGE = 3;
+constexpr int IMG_PF = 2;
+constexpr int IMG_NADJ = 9;  // f1, f2, m1, m2, m3, m4, irho, rx, ry with a halo of 4
+constexpr size_t IMG_P = (size_t)PH * PW * sizeof(float);
+constexpr size_t IMG_A = (size_t)IH * IW * sizeof(float);
+constexpr size_t IMG_STAGE = 2 * IMG_P + IMG_NADJ * IMG_A;
+constexpr size_t IMG_T1 = (size_t)2 * TY * IW * sizeof(float);  // x-type tiles: rows y0.., cols x0-4..
+constexpr size_t IMG_T2 = (size_t)2 * IH * TX * sizeof(float);  // y-type tiles: rows y0-4.., cols x0..
+constexpr size_t IMG_SMEM = IMG_NSTAGE * IMG_STAGE + 2 * IMG_T1 + 2 * IMG_T2 + IMG_NSTAGE * sizeof(uint64_t);
+
+struct ImgMaps {
+    CUtensorMap snap;            // 4D over the store: (nx, ny, nz, 4*nsnap), box PW x PH
+    CUtensorMap a[IMG_NADJ];     // box IW x IH over halo'd volumes
+};
+enum { A_P = 0, A_Q, A_M1, A_M2, A_M3, A_M4, A_IR, A_RX, A_RY };
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
+                                            uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(saddr(bar))
+        : "memory");
+}
+
+// adjoint temporary rho*(s1 + r^2 h1), rho*(s2 + r^2 h2) at staging offset k (halo-4 tile)
+__device__ __forceinline__ float2 img_adj(const float* A, int k, float ra)
+{
+    const float p = A[A_P * IH * IW + k], q = A[A_Q * IH * IW + k];
+    const float a1 = A[A_M1 * IH * IW + k], a2 = A[A_M2 * IH * IW + k], a3 = A[A_M3 * IH * IW + k],
+                a4 = A[A_M4 * IH * IW + k];
+    const float rho = 1.0f / A[A_IR * IH * IW + k];
+    const float rr = ra * ra;
+    const float lx = (a4 - a1) * p - a2 * q;
+    const float lz = a2 * p + (a3 - a4) * q;
+    return make_float2(rho * (a1 * p + a2 * q + rr * lx), rho * (a4 * q + rr * lz));
+}
+
+template <bool TTI>
+__global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ ImgMaps tm, const ImgParams a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* stage = reinterpret_cast<float*>(smem);
+    unsigned char* sp = smem + IMG_NSTAGE * IMG_STAGE;
+    float* fdx = reinterpret_cast<float*>(sp);
+    sp += IMG_T1;
+    float* axs = reinterpret_cast<float*>(sp);
+    sp += IMG_T1;
+    float* fdy = reinterpret_cast<float*>(sp);
+    sp += IMG_T2;
+    float* ays = reinterpret_cast<float*>(sp);
+    sp += IMG_T2;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sp);
+
+    const Layout& L = a.L;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int x0 = L.ixbeg + blockIdx.x * TX, y0 = L.iybeg + blockIdx.y * TY;
+    const int xd0 = blockIdx.x * TX, yd0 = blockIdx.y * TY;  // dense (interior) origin
+    const int zs = L.izbeg + blockIdx.z * a.bz;
+    const int ze = min(zs + a.bz - 1, L.izend);
+    const int ntot = ze - zs + 1 + 2 * LAG;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool owner = (x <= L.ixend) && (y <= L.iyend);
+    const int nx = L.nx(), ny = L.ny();
+    bool dead = false;
+    constexpr int NADJ = TTI ? IMG_NADJ : A_RX;
+    constexpr uint32_t TX_BYTES = (uint32_t)(2 * IMG_P + NADJ * IMG_A);
+
+    if (tid == 0) {
+        for (int s = 0; s < IMG_NSTAGE; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    // plane z of the stored p/q: dense z = z - izbeg; above the surface the
+    // free surface mirrors it (2*izbeg - z), without one it is zero halo.
+    auto issue = [&](int t) {
+        const int s = t % IMG_NSTAGE, z = zs - LAG + t;
+        float* dst = stage + (size_t)s * (IMG_STAGE / sizeof(float));
+        mbar_expect_tx(&bars[s], TX_BYTES);
+        int zd = z - L.izbeg;
+        if (a.fs && zd < 0) zd = -zd;
+        tma_load_4d(dst, &tm.snap, xd0 - 8, yd0 - 8, zd, 4 * a.slot + 2, &bars[s]);
+        tma_load_4d(dst + PH * PW, &tm.snap, xd0 - 8, yd0 - 8, zd, 4 * a.slot + 3, &bars[s]);
+        float* adst = dst + 2 * PH * PW;
+#pragma unroll
+        for (int k = 0; k < NADJ; ++k) tma_load_3d(adst + k * IH * IW, &tm.a[k], x0 - 4, y0 - 4, z, &bars[s]);
+    };
+    if (tid == 0)
+        for (int t = 0; t < IMG_PF && t < ntot; ++t) issue(t);
+
+    float dzq1[8], dzq2[8];  // D- partial sums of the stored p/q, positions L-3 .. L+4
+    float fz1[8], fz2[8];    // forward z derivatives, positions L-10 .. L-3
+    float az1q[12], az2q[12];  // adjoint z temporaries, planes L-11 .. L
+    float rxy[8];            // x+y part of the gradient rhs, outputs L-7 .. L
+    float irq[8];            // buoyancy of this column, planes L-7 .. L
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dzq1[j] = dzq2[j] = fz1[j] = fz2[j] = rxy[j] = irq[j] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 12; ++j) az1q[j] = az2q[j] = 0.0f;
+
+    for (int t = 0; t < ntot; ++t) {
+        __syncthreads();  // the x/y tiles of plane L-1 have been read by every thread
+        if (tid == 0 && t + IMG_PF < ntot) {
+            fence_proxy_async();
+            issue(t + IMG_PF);
+        }
+        const int s = t % IMG_NSTAGE;
+        const int Lz = zs - LAG + t;
+        mbar_wait(&bars[s], (uint32_t)((t / IMG_NSTAGE) & 1), a.err, dead);
+        float* st = stage + (size_t)s * (IMG_STAGE / sizeof(float));
+        const bool mirrored = a.fs && Lz < L.izbeg;
+        if (mirrored) {  // block-uniform
+            for (int e = tid; e < 2 * PH * PW; e += NT) st[e] = -st[e];
+            __syncthreads();
+        }
+        const float* P1 = st;
+        const float* P2 = st + PH * PW;
+        const float* A = st + 2 * PH * PW;
+        const int kc = (ty + 4) * IW + tx + 4;  // this column in a halo-4 tile
+
+        // (1) forward x/y derivatives of the stored p/q (fwd_drv) and the
+        //     adjoint x/y temporaries of plane L
+        for (int e = tid; e < 2 * TY * IW; e += NT) {
+            const int f = e / (TY * IW), r = (e / IW) % TY, c = e % IW;  // x = x0-4+c, y = y0+r
+            const float* Pf = f ? P2 : P1;
+            float acc = 0.0f;
+#pragma unroll
+            for (int i = 1; i <= 4; ++i) acc += c1(i) * (Pf[(r + 8) * PW + c + 3 + i] - Pf[(r + 8) * PW + c + 4 - i]);
+            acc *= a.hx;
+            const int gx = x0 - 4 + c;
+            const float v = acc * A[A_IR * IH * IW + (r + 4) * IW + c];
+            fdx[e] = (gx >= L.ixbeg && gx <= L.ixend) ? v : 0.0f;
+            if (f == 0) {
+                const int k = (r + 4) * IW + c;
+                const float2 t2 = img_adj(A, k, TTI ? A[A_RX * IH * IW + k] : 0.0f);
+                axs[e] = t2.x;
+                axs[TY * IW + e] = t2.y;
+            }
+        }
+        for (int e = tid; e < 2 * IH * TX; e += NT) {
+            const int f = e / (IH * TX), r = (e / TX) % IH, c = e % TX;  // y = y0-4+r, x = x0+c
+            const float* Pf = f ? P2 : P1;
+            float acc = 0.0f;
+#pragma unroll
+            for (int i = 1; i <= 4; ++i)
+                acc += c1(i) * (Pf[(r + 3 + i) * PW + c + 8] - Pf[(r + 4 - i) * PW + c + 8]);
+            acc *= a.hy;
+            const int gy = y0 - 4 + r;
+            const float v = acc * A[A_IR * IH * IW + r * IW + c + 4];
+            fdy[e] = (gy >= L.iybeg && gy <= L.iyend) ? v : 0.0f;
+            if (f == 0) {
+                const int k = r * IW + c + 4;
+                const float2 t2 = img_adj(A, k, TTI ? A[A_RY * IH * IW + k] : 0.0f);
+                ays[e] = t2.x;
+                ays[IH * TX + e] = t2.y;
+            }
+        }
+        // (2) column values: z temporaries, buoyancy, D- z stage of the stored p/q
+        {
+            const int64_t gc = L.idx(min(x, L.ldimx - 1), min(y, L.ldimy - 1), min(max(Lz, 0), L.ldimz - 1));
+            const float vrz = TTI ? __ldg(a.rz + gc) : 1.0f;
+            const float2 t2 = img_adj(A, kc, vrz);
+#pragma unroll
+            for (int j = 0; j < 11; ++j) {
+                az1q[j] = az1q[j + 1];
+                az2q[j] = az2q[j + 1];
+            }
+            az1q[11] = t2.x;
+            az2q[11] = t2.y;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) irq[j] = irq[j + 1];
+            irq[7] = A[A_IR * IH * IW + kc];
+            const float v1 = P1[(ty + 8) * PW + tx + 8], v2 = P2[(ty + 8) * PW + tx + 8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float cf = dminus_coef(j);
+                dzq1[j] = dzq1[j] + cf * v1;
+                dzq2[j] = dzq2[j] + cf * v2;
+            }
+            const int zp = Lz - 3;
+            const bool valid = (zp >= L.izbeg + (a.fs ? 1 : 0)) && zp <= L.izend;
+            const float ir3 = irq[4];  // plane L-3
+            const float n1 = valid ? (dzq1[0] * a.hz) * ir3 : 0.0f;
+            const float n2 = valid ? (dzq2[0] * a.hz) * ir3 : 0.0f;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) {
+                fz1[j] = fz1[j + 1];
+                fz2[j] = fz2[j + 1];
+                dzq1[j] = dzq1[j + 1];
+                dzq2[j] = dzq2[j + 1];
+            }
+            fz1[7] = n1;
+            fz2[7] = n2;
+            dzq1[7] = 0.0f;
+            dzq2[7] = 0.0f;
+        }
+        __syncthreads();  // x/y tiles of plane L ready; staging slot s fully consumed
+
+        // (3) x+y part of the gradient rhs at plane L (compute_xy_contributions
+        //     of kernel_type2_grad.cu:314-342 and :435-439) and the Vp image
+        {
+            const float* X1 = fdx;
+            const float* X2 = fdx + TY * IW;
+            const float* AX1 = axs;
+            const float* AX2 = axs + TY * IW;
+            const float* Y1 = fdy;
+            const float* Y2 = fdy + IH * TX;
+            const float* AY1 = ays;
+            const float* AY2 = ays + IH * TX;
+            const int cx = ty * IW + tx + 4;    // x in the x-type tiles
+            const int cy = (ty + 4) * TX + tx;  // y in the y-type tiles
+            float dfx1 = 0, dfx2 = 0, dfy1 = 0, dfy2 = 0, dax1 = 0, dax2 = 0, day1 = 0, day2 = 0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const float c = cs(r);
+                dfx1 += c * (X1[cx + r + 1] - X1[cx - r]);
+                dfx2 += c * (X2[cx + r + 1] - X2[cx - r]);
+                dfy1 += c * (Y1[cy + (r + 1) * TX] - Y1[cy - r * TX]);
+                dfy2 += c * (Y2[cy + (r + 1) * TX] - Y2[cy - r * TX]);
+                dax1 += c * (AX1[cx + r] - AX1[cx - r - 1]);
+                dax2 += c * (AX2[cx + r] - AX2[cx - r - 1]);
+                day1 += c * (AY1[cy + r * TX] - AY1[cy - (r + 1) * TX]);
+                day2 += c * (AY2[cy + r * TX] - AY2[cy - (r + 1) * TX]);
+            }
+            dfx1 *= a.hx;
+            dfx2 *= a.hx;
+            dfy1 *= a.hy;
+            dfy2 *= a.hy;
+            dax1 *= a.hx;
+            dax2 *= a.hx;
+            day1 *= a.hy;
+            day2 *= a.hy;
+            const float v = AX1[cx] * dfx1 + AX2[cx] * dfx2 + AY1[cy] * dfy1 + AY2[cy] * dfy2 + dax1 * X1[cx] +
+                            dax2 * X2[cx] + day1 * Y1[cy] + day2 * Y2[cy];
+#pragma unroll
+            for (int j = 0; j < 7; ++j) rxy[j] = rxy[j + 1];
+            rxy[7] = v;
+            if (owner && Lz >= zs && Lz <= ze) {
+                const int64_t gi = L.idx(x, y, Lz);
+                const int64_t d = ((int64_t)(Lz - L.izbeg) * ny + (y - L.iybeg)) * nx + (x - L.ixbeg);
+                const float s3 = __ldg(a.snap3 + d), s4 = __ldg(a.snap4 + d);
+                a.gvp[d] += __ldg(a.f3 + gi) * s3 + __ldg(a.f4 + gi) * s4;
+            }
+        }
+        // (4) output plane L-7: z terms and the density gradient
+        const int z = Lz - LAG;
+        if (z >= zs && owner) {
+            float q1[8], q2[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                q1[j] = fz1[j];
+                q2[j] = fz2[j];
+            }
+            if (a.fs) {
+                resolve_dz(q1, z - L.izbeg);
+                resolve_dz(q2, z - L.izbeg);
+            }
+            // q[j] is position z-3+j; az*q[j] is plane z-4+j
+            float dfz1 = 0, dfz2 = 0, daz1 = 0, daz2 = 0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const float c = cs(r);
+                dfz1 += c * (q1[4 + r] - q1[3 - r]);
+                dfz2 += c * (q2[4 + r] - q2[3 - r]);
+                daz1 += c * (az1q[4 + r] - az1q[3 - r]);
+                daz2 += c * (az2q[4 + r] - az2q[3 - r]);
+            }
+            dfz1 *= a.hz;
+            dfz2 *= a.hz;
+            daz1 *= a.hz;
+            daz2 *= a.hz;
+            const float rhs = rxy[0] + az1q[4] * dfz1 + az2q[4] * dfz2 + daz1 * q1[3] + daz2 * q2[3];
+            const int64_t d = ((int64_t)(z - L.izbeg) * ny + (y - L.iybeg)) * nx + (x - L.ixbeg);
+            a.grho[d] += -irq[0] * rhs;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host side: tensor maps and launchers.
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
@@ -1022,6 +1323,84 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
             attr_set[1] = true;
         }
         k_fused_adjoint<true><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
+    }
+    return launch_status();
+}
+
+namespace {
+// 4D FP32 tensor map over the dense snapshot store (nx, ny, nz, 4*nsnap).
+bool make_store_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, int nvol, int bx, int by)
+{
+    auto fn = encode_fn();
+    if (!fn || !base) return false;
+    cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nvol};
+    cuuint64_t strides[3] = {(cuuint64_t)nx * sizeof(float), (cuuint64_t)nx * ny * sizeof(float),
+                             (cuuint64_t)nx * ny * nz * sizeof(float)};
+    cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+} // namespace
+
+bool fused_image_supported(const Layout& L) { return layout_supported(L) && L.nx() % 4 == 0; }
+
+int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
+{
+    if (!fused_image_supported(L) || !s.store || s.slot < 0 || s.slot >= s.nsnap) return TTI_EINVAL;
+    ImgMaps tm;
+    {
+        static std::mutex mu;
+        static const float* cached_base = nullptr;
+        static int cached_dims[4] = {0, 0, 0, 0};
+        static CUtensorMap cached;
+        std::lock_guard<std::mutex> lk(mu);
+        const int dims[4] = {L.nx(), L.ny(), L.nz(), 4 * s.nsnap};
+        if (cached_base != s.store || std::memcmp(dims, cached_dims, sizeof(dims)) != 0) {
+            if (!make_store_map(&cached, s.store, L.nx(), L.ny(), L.nz(), 4 * s.nsnap, PW, PH)) return TTI_ELAUNCH;
+            cached_base = s.store;
+            std::memcpy(cached_dims, dims, sizeof(dims));
+        }
+        tm.snap = cached;
+    }
+    const float* arr[IMG_NADJ] = {s.adj1, s.adj2, s.m.m1, s.m.m2, s.m.m3, s.m.m4, s.m.irho, s.m.rx, s.m.ry};
+    for (int k = 0; k < IMG_NADJ; ++k)
+        if (!get_map(&tm.a[k], arr[k], L, IW, IH)) return TTI_ELAUNCH;
+    ImgParams a{};
+    a.f3 = s.adj3;
+    a.f4 = s.adj4;
+    a.rz = s.m.rz;
+    a.irho = s.m.irho;
+    const int64_t nin = (int64_t)L.nx() * L.ny() * L.nz();
+    a.snap3 = s.store + (size_t)s.slot * 4 * nin;
+    a.snap4 = a.snap3 + nin;
+    a.gvp = s.grad_vp;
+    a.grho = s.grad_rho;
+    a.L = L;
+    a.bz = pick_bz(L);
+    a.fs = s.free_surface;
+    a.slot = s.slot;
+    a.hx = 1.0 / s.dx;
+    a.hy = 1.0 / s.dy;
+    a.hz = 1.0 / s.dz;
+    a.err = err_word();
+    if (!a.err) return TTI_ENOMEM;
+    dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
+    static bool attr_set[2] = {false, false};
+    if (s.vti) {
+        if (!attr_set[0]) {
+            cudaFuncSetAttribute(k_fused_image<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IMG_SMEM);
+            attr_set[0] = true;
+        }
+        k_fused_image<false><<<grid, dim3(TX, TY), IMG_SMEM, st>>>(tm, a);
+    } else {
+        if (!attr_set[1]) {
+            cudaFuncSetAttribute(k_fused_image<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IMG_SMEM);
+            attr_set[1] = true;
+        }
+        k_fused_image<true><<<grid, dim3(TX, TY), IMG_SMEM, st>>>(tm, a);
     }
     return launch_status();
 }

@@ -70,6 +70,28 @@ struct AdjStepArgs {
 };
 int launch_fused_adjoint(const Layout& L, const AdjStepArgs& a, cudaStream_t st);
 
+// Fused imaging at a snapshot step (tti_fused.cu): Vp image from the adjoint
+// pdot/qdot and the stored pdot/qdot, density gradient from the stored p/q
+// (forward derivatives formed on the fly) and the adjoint p/q.  The store is
+// nsnap slots of four dense interior volumes (pdot, qdot, p, q).
+struct ImageArgs {
+    const float* adj1;
+    const float* adj2;
+    const float* adj3;
+    const float* adj4;
+    const float* store;
+    int nsnap;
+    int slot;
+    Model m;
+    float* grad_vp;   // dense nx*ny*nz
+    float* grad_rho;  // dense nx*ny*nz
+    int free_surface;
+    int vti;
+    double dx, dy, dz;
+};
+bool fused_image_supported(const Layout& L);
+int launch_fused_image(const Layout& L, const ImageArgs& a, cudaStream_t st);
+
 // Status of the bounded waits inside the fused kernels since the last call
 // (TTI_ETIMEOUT if any gave up); synchronizes the stream.
 int fused_wait_status(cudaStream_t st);

@@ -737,7 +737,28 @@ static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device
         if (n % c.xcorr_step == 0) {
             const float* slot = s->snaps + (size_t)(n / c.xcorr_step) * 4 * s->ninterior;
             mark_begin(s, 2, st);
-            rc = image_per_kernel(s, slot, st);
+            if (fused && fused_image_supported(L)) {
+                ImageArgs ia{};
+                ia.adj1 = s->f1;
+                ia.adj2 = s->f2;
+                ia.adj3 = s->f3;
+                ia.adj4 = s->f4;
+                ia.store = s->snaps;
+                ia.nsnap = s->nsnap;
+                ia.slot = n / c.xcorr_step;
+                ia.m = model_of(s);
+                ia.grad_vp = s->grad_vp;
+                ia.grad_rho = s->grad_rho;
+                ia.free_surface = c.free_surface;
+                ia.vti = s->vti ? 1 : 0;
+                ia.dx = c.dx;
+                ia.dy = c.dy;
+                ia.dz = c.dz;
+                rc = launch_fused_image(L, ia, st);
+                s->launches++;
+            } else {
+                rc = image_per_kernel(s, slot, st);
+            }
             mark_end(s, st);
             if (rc) return rc;
         }
