@@ -208,14 +208,16 @@ __global__ void __launch_bounds__(NT, 1)
 
     const int vc = (tx + 8), vr = (ty + 8);  // this column inside a p/q tile
 
+    int s = 0;           // ring slot of plane t
+    uint32_t phase = 0;  // mbarrier parity of slot s for this use
+    auto back = [&](int k) { const int v = s - k; return v < 0 ? v + FWD_NS : v; };
     for (int t = 0; t < ntot; ++t) {
         __syncthreads();  // every thread is done with iteration t-1
         if (tid == 0 && t + FWD_PF < ntot) {
             fence_proxy_async();
             issue(t + FWD_PF);
         }
-        const int s = t % FWD_NS;
-        mbar_wait(&bars[s], (uint32_t)((t / FWD_NS) & 1), a.err, dead);
+        mbar_wait(&bars[s], phase, a.err, dead);
         const int Lz = zs - LAG + t;
         const float* P1 = ring + (size_t)s * 2 * PH * PW;
         const float* P2 = P1 + PH * PW;
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(NT, 1)
         {
             const int zp = Lz - 3;
             const bool valid = (zp >= L.izbeg + (a.fs ? 1 : 0)) && zp <= L.izend;
-            const float* I3 = iring + (size_t)((t + FWD_NS - 3) % FWD_NS) * IH * IW;
+            const float* I3 = iring + (size_t)back(3) * IH * IW;
             const float ir3 = I3[(ty + 4) * IW + tx + 4];
             const float n1 = valid ? (dzq1[0] * a.invdz) * ir3 : 0.0f;
             const float n2 = valid ? (dzq2[0] * a.invdz) * ir3 : 0.0f;
@@ -257,7 +259,7 @@ __global__ void __launch_bounds__(NT, 1)
             for (int m = -4; m <= 4; ++m) {
                 if (m == 0) continue;
                 const float c = c2(m < 0 ? -m : m);
-                const float* Q1 = ring + (size_t)((t + FWD_NS - 4 + m) % FWD_NS) * 2 * PH * PW;
+                const float* Q1 = ring + (size_t)back(4 - m) * 2 * PH * PW;
                 const float* Q2 = Q1 + PH * PW;
                 mz[0] += c * (Q1[vr * PW + vc + m] - Q1[vr * PW + vc - m]);
                 mz[1] += c * (Q2[vr * PW + vc + m] - Q2[vr * PW + vc - m]);
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(NT, 1)
         // (c) output plane L-7
         const int z = Lz - LAG;
         if (z >= zs) {  // block-uniform
-            const int s7 = (t + FWD_NS - LAG) % FWD_NS;
+            const int s7 = back(LAG);
             const float* O1 = ring + (size_t)s7 * 2 * PH * PW;
             const float* I7 = iring + (size_t)s7 * IH * IW;
             // issue the point-wise loads of this cell early
@@ -297,29 +299,37 @@ __global__ void __launch_bounds__(NT, 1)
                 sz = __ldg(a.abz + z);
             }
             // buoyancy-scaled first derivatives of plane z on the halo'd tile
-            for (int e = tid; e < 2 * TY * IW; e += NT) {
-                const int f = e / (TY * IW), r = (e / IW) % TY, c = e % IW;
-                const float* Pf = O1 + f * PH * PW;
-                const int gx = x0 - 4 + c;
-                float acc = 0.0f;
+            // dxs[f][r][c]: x = x0-4+c, y = y0+r;  dys[f][r][c]: x = x0+c, y = y0-4+r
+            auto dx_at = [&](int r, int c) {
+                const bool in = (x0 - 4 + c >= L.ixbeg) && (x0 - 4 + c <= L.ixend);
+                const float irv = I7[(r + 4) * IW + c];
 #pragma unroll
-                for (int i = 1; i <= 4; ++i) acc += c1(i) * (Pf[(r + 8) * PW + c + 3 + i] - Pf[(r + 8) * PW + c + 4 - i]);
-                acc *= a.invdx;
-                const float v = acc * I7[(r + 4) * IW + c];
-                dxs[e] = (gx >= L.ixbeg && gx <= L.ixend) ? v : 0.0f;
-            }
-            for (int e = tid; e < 2 * IH * TX; e += NT) {
-                const int f = e / (IH * TX), r = (e / TX) % IH, c = e % TX;
-                const float* Pf = O1 + f * PH * PW;
-                const int gy = y0 - 4 + r;
-                float acc = 0.0f;
+                for (int f = 0; f < 2; ++f) {
+                    const float* Pr = O1 + f * PH * PW + (r + 8) * PW + c + 4;
+                    float acc = 0.0f;
 #pragma unroll
-                for (int i = 1; i <= 4; ++i)
-                    acc += c1(i) * (Pf[(r + 3 + i) * PW + c + 8] - Pf[(r + 4 - i) * PW + c + 8]);
-                acc *= a.invdy;
-                const float v = acc * I7[r * IW + c + 4];
-                dys[e] = (gy >= L.iybeg && gy <= L.iyend) ? v : 0.0f;
-            }
+                    for (int i = 1; i <= 4; ++i) acc += c1(i) * (Pr[i - 1] - Pr[-i]);
+                    acc *= a.invdx;
+                    dxs[f * TY * IW + r * IW + c] = in ? acc * irv : 0.0f;
+                }
+            };
+            auto dy_at = [&](int r, int c) {
+                const bool in = (y0 - 4 + r >= L.iybeg) && (y0 - 4 + r <= L.iyend);
+                const float irv = I7[r * IW + c + 4];
+#pragma unroll
+                for (int f = 0; f < 2; ++f) {
+                    const float* Pc = O1 + f * PH * PW + (r + 4) * PW + c + 8;
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int i = 1; i <= 4; ++i) acc += c1(i) * (Pc[(i - 1) * PW] - Pc[-i * PW]);
+                    acc *= a.invdy;
+                    dys[f * IH * TX + r * TX + c] = in ? acc * irv : 0.0f;
+                }
+            };
+            dx_at(ty, tx);
+            if (tx < IW - TX) dx_at(ty, tx + TX);
+            dy_at(ty, tx);
+            if (ty < IH - TY) dy_at(ty + TY, tx);
             __syncthreads();
             if (owner) {
                 float xx1 = 0, xx2 = 0, yy1 = 0, yy2 = 0;
@@ -353,7 +363,7 @@ __global__ void __launch_bounds__(NT, 1)
                 zz1 *= a.invdz;
                 zz2 *= a.invdz;
                 const float ir = I7[(ty + 4) * IW + tx + 4];
-                const float rho = 1.0f / ir;
+                const float rho = __frcp_rn(ir);
                 float r3, r4;
                 const float* O2 = O1 + PH * PW;
                 if constexpr (TTI) {
@@ -439,6 +449,10 @@ __global__ void __launch_bounds__(NT, 1)
                 mq[2][c] = mz[c];
             }
         }
+        if (++s == FWD_NS) {
+            s = 0;
+            phase ^= 1u;
+        }
     }
 }
 
@@ -507,7 +521,7 @@ __device__ __forceinline__ Base base_at(const float* st, int k)
     b.h1 = (-a1 + a4) * p - a2 * q;
     b.s2 = a4 * q;
     b.h2 = a2 * p + (-a4 + a3) * q;
-    b.rho = 1.0f / st[S_IR * PH * PW + k];
+    b.rho = __frcp_rn(st[S_IR * PH * PW + k]);
     return b;
 }
 
@@ -574,62 +588,71 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
 #pragma unroll
     for (int j = 0; j < 4; ++j) irq[j] = 0.0f;
 
+    int s = 0;
+    uint32_t phase = 0;
     for (int t = 0; t < ntot; ++t) {
         // Stage (t+2)%3 was last read in iteration t-1, before its final barrier.
         if (tid == 0 && t + ADJ_PF < ntot) {
             fence_proxy_async();
             issue(t + ADJ_PF);
         }
-        const int s = t % ADJ_NSTAGE;
         const int Lz = zs - LAG + t;
-        mbar_wait(&bars[s], (uint32_t)((t / ADJ_NSTAGE) & 1), a.err, dead);
+        mbar_wait(&bars[s], phase, a.err, dead);
         const float* st = stage + (size_t)s * (ADJ_STAGE / sizeof(float));
         const float* srz = st + ADJ_NARR * PH * PW;  // rz tile, origin (x0-4, y0-4)
 
-        // (1) temporaries of plane L
-        for (int e = tid; e < TY * PW; e += NT) {  // xx: rows y0.., cols x0-8..
-            const int r = e / PW, c = e % PW;
-            const int k = (r + 8) * PW + c;
+        // (1) temporaries of plane L (kernel_type2_grad_snap.cu:98-129), each
+        //     staging position visited once: position (r, c) of the halo-8
+        //     tile (y = y0-8+r, x = x0-8+c) feeds
+        //       xx if 8<=r<24;  yy if 8<=c<40;  xy if 4<=r<28 and 4<=c<44;
+        //       yz if 4<=r<28 and 8<=c<40;  zx if 8<=r<24 and 4<=c<44.
+        auto temps_at = [&](int r, int c) {
+            const bool nx_ = (r >= 8 && r < 8 + TY), ny_ = (c >= 8 && c < 8 + TX);
+            const bool in4 = (r >= 4 && r < PH - 4 && c >= 4 && c < PW - 4);
+            if (!(nx_ || ny_ || (TTI && in4))) return;
+            const int k = r * PW + c;
             const Base b = base_at(st, k);
-            const float vr = TTI ? st[S_RX * PH * PW + k] : 0.0f;
-            const float rr = vr * vr;
-            txx[e] = b.rho * (b.s1 + rr * b.h1);
-            txx[TY * PW + e] = b.rho * (b.s2 + rr * b.h2);
-        }
-        for (int e = tid; e < PH * TX; e += NT) {  // yy: rows y0-8.., cols x0..
-            const int r = e / TX, c = e % TX;
-            const int k = r * PW + c + 8;
-            const Base b = base_at(st, k);
-            const float vr = TTI ? st[S_RY * PH * PW + k] : 0.0f;
-            const float rr = vr * vr;
-            tyy[e] = b.rho * (b.s1 + rr * b.h1);
-            tyy[PH * TX + e] = b.rho * (b.s2 + rr * b.h2);
-        }
-        if constexpr (TTI) {
-            for (int e = tid; e < IH * IW; e += NT) {  // xy: rows y0-4.., cols x0-4..
-                const int r = e / IW, c = e % IW;
-                const int k = (r + 4) * PW + c + 4;
-                const Base b = base_at(st, k);
-                const float w = 2.0f * st[S_RX * PH * PW + k] * st[S_RY * PH * PW + k];
-                txy[e] = w * b.h1;
-                txy[IH * IW + e] = w * b.h2;
+            const float vrx = TTI ? st[S_RX * PH * PW + k] : 0.0f;
+            const float vry = TTI ? st[S_RY * PH * PW + k] : 0.0f;
+            if (nx_) {
+                const float rr = vrx * vrx;
+                const int e = (r - 8) * PW + c;
+                txx[e] = b.rho * (b.s1 + rr * b.h1);
+                txx[TY * PW + e] = b.rho * (b.s2 + rr * b.h2);
             }
-            for (int e = tid; e < IH * TX; e += NT) {  // yz: rows y0-4.., cols x0..
-                const int r = e / TX, c = e % TX;
-                const int k = (r + 4) * PW + c + 8;
-                const Base b = base_at(st, k);
-                const float w = 2.0f * st[S_RY * PH * PW + k] * srz[r * IW + c + 4];
-                tyz[e] = w * b.h1;
-                tyz[IH * TX + e] = w * b.h2;
+            if (ny_) {
+                const float rr = vry * vry;
+                const int e = r * TX + c - 8;
+                tyy[e] = b.rho * (b.s1 + rr * b.h1);
+                tyy[PH * TX + e] = b.rho * (b.s2 + rr * b.h2);
             }
-            for (int e = tid; e < TY * IW; e += NT) {  // zx: rows y0.., cols x0-4..
-                const int r = e / IW, c = e % IW;
-                const int k = (r + 8) * PW + c + 4;
-                const Base b = base_at(st, k);
-                const float w = 2.0f * srz[(r + 4) * IW + c] * st[S_RX * PH * PW + k];
-                tzx[e] = w * b.h1;
-                tzx[TY * IW + e] = w * b.h2;
+            if constexpr (TTI) {
+                if (in4) {
+                    const float vrz = srz[(r - 4) * IW + c - 4];
+                    const float wxy = 2.0f * vrx * vry;
+                    const int exy = (r - 4) * IW + c - 4;
+                    txy[exy] = wxy * b.h1;
+                    txy[IH * IW + exy] = wxy * b.h2;
+                    if (ny_) {
+                        const float w = 2.0f * vry * vrz;
+                        const int e = (r - 4) * TX + c - 8;
+                        tyz[e] = w * b.h1;
+                        tyz[IH * TX + e] = w * b.h2;
+                    }
+                    if (nx_) {
+                        const float w = 2.0f * vrz * vrx;
+                        const int e = (r - 8) * IW + c - 4;
+                        tzx[e] = w * b.h1;
+                        tzx[TY * IW + e] = w * b.h2;
+                    }
+                }
             }
+        };
+        temps_at(ty, tx);
+        temps_at(ty + TY, tx);
+        if (tx < PW - TX) {
+            temps_at(ty, tx + TX);
+            temps_at(ty + TY, tx + TX);
         }
         // this column's zz temporary and buoyancy at plane L
         const int kc = (ty + 8) * PW + tx + 8;
@@ -647,27 +670,35 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
         __syncthreads();  // temporaries of plane L are ready
 
         // (2) buoyancy-scaled x/y derivatives of plane L (compute_xy_contributions)
-        for (int e = tid; e < 2 * TY * IW; e += NT) {
-            const int f = e / (TY * IW), r = (e / IW) % TY, c = e % IW;  // x = x0-4+c, y = y0+r
-            const float* T = txx + f * TY * PW + r * PW;
+        // dxs[f][r][c]: x = x0-4+c, y = y0+r;  dys[f][r][c]: x = x0+c, y = y0-4+r
+        auto dx_at = [&](int r, int c) {
+            const bool in = (x0 - 4 + c >= L.ixbeg) && (x0 - 4 + c <= L.ixend);
             const float irv = st[S_IR * PH * PW + (r + 8) * PW + c + 4];
-            float acc = 0.0f;
 #pragma unroll
-            for (int i = 1; i <= 4; ++i) acc += (a.invdx * c1(i)) * (T[c + 3 + i] - T[c + 4 - i]) * irv;
-            const int gx = x0 - 4 + c;
-            dxs[e] = (gx >= L.ixbeg && gx <= L.ixend) ? acc : 0.0f;
-        }
-        for (int e = tid; e < 2 * IH * TX; e += NT) {
-            const int f = e / (IH * TX), r = (e / TX) % IH, c = e % TX;  // y = y0-4+r, x = x0+c
-            const float* T = tyy + f * PH * TX;
+            for (int f = 0; f < 2; ++f) {
+                const float* T = txx + f * TY * PW + r * PW + c + 4;
+                float acc = 0.0f;
+#pragma unroll
+                for (int i = 1; i <= 4; ++i) acc += (a.invdx * c1(i)) * (T[i - 1] - T[-i]) * irv;
+                dxs[f * TY * IW + r * IW + c] = in ? acc : 0.0f;
+            }
+        };
+        auto dy_at = [&](int r, int c) {
+            const bool in = (y0 - 4 + r >= L.iybeg) && (y0 - 4 + r <= L.iyend);
             const float irv = st[S_IR * PH * PW + (r + 4) * PW + c + 8];
-            float acc = 0.0f;
 #pragma unroll
-            for (int i = 1; i <= 4; ++i)
-                acc += (a.invdy * c1(i)) * (T[(r + 3 + i) * TX + c] - T[(r + 4 - i) * TX + c]) * irv;
-            const int gy = y0 - 4 + r;
-            dys[e] = (gy >= L.iybeg && gy <= L.iyend) ? acc : 0.0f;
-        }
+            for (int f = 0; f < 2; ++f) {
+                const float* T = tyy + f * PH * TX + (r + 4) * TX + c;
+                float acc = 0.0f;
+#pragma unroll
+                for (int i = 1; i <= 4; ++i) acc += (a.invdy * c1(i)) * (T[(i - 1) * TX] - T[-i * TX]) * irv;
+                dys[f * IH * TX + r * TX + c] = in ? acc : 0.0f;
+            }
+        };
+        dx_at(ty, tx);
+        if (tx < IW - TX) dx_at(ty, tx + TX);
+        dy_at(ty, tx);
+        if (ty < IH - TY) dy_at(ty + TY, tx);
         // (3) D- z stage (compute_z_contributionsdtd), completes position L-3
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -816,6 +847,10 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
         }
         mx1[11] = 0.0f;
         mx2[11] = 0.0f;
+        if (++s == ADJ_NSTAGE) {
+            s = 0;
+            phase ^= 1u;
+        }
     }
 }
 
@@ -871,7 +906,7 @@ __device__ __forceinline__ float2 img_adj(const float* A, int k, float ra)
     const float p = A[A_P * IH * IW + k], q = A[A_Q * IH * IW + k];
     const float a1 = A[A_M1 * IH * IW + k], a2 = A[A_M2 * IH * IW + k], a3 = A[A_M3 * IH * IW + k],
                 a4 = A[A_M4 * IH * IW + k];
-    const float rho = 1.0f / A[A_IR * IH * IW + k];
+    const float rho = __frcp_rn(A[A_IR * IH * IW + k]);
     const float rr = ra * ra;
     const float lx = (a4 - a1) * p - a2 * q;
     const float lz = a2 * p + (a3 - a4) * q;
@@ -941,15 +976,16 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
 #pragma unroll
     for (int j = 0; j < 12; ++j) az1q[j] = az2q[j] = 0.0f;
 
+    int s = 0;
+    uint32_t phase = 0;
     for (int t = 0; t < ntot; ++t) {
         __syncthreads();  // the x/y tiles of plane L-1 have been read by every thread
         if (tid == 0 && t + IMG_PF < ntot) {
             fence_proxy_async();
             issue(t + IMG_PF);
         }
-        const int s = t % IMG_NSTAGE;
         const int Lz = zs - LAG + t;
-        mbar_wait(&bars[s], (uint32_t)((t / IMG_NSTAGE) & 1), a.err, dead);
+        mbar_wait(&bars[s], phase, a.err, dead);
         float* st = stage + (size_t)s * (IMG_STAGE / sizeof(float));
         const bool mirrored = a.fs && Lz < L.izbeg;
         if (mirrored) {  // block-uniform
@@ -962,42 +998,46 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
         const int kc = (ty + 4) * IW + tx + 4;  // this column in a halo-4 tile
 
         // (1) forward x/y derivatives of the stored p/q (fwd_drv) and the
-        //     adjoint x/y temporaries of plane L
-        for (int e = tid; e < 2 * TY * IW; e += NT) {
-            const int f = e / (TY * IW), r = (e / IW) % TY, c = e % IW;  // x = x0-4+c, y = y0+r
-            const float* Pf = f ? P2 : P1;
-            float acc = 0.0f;
+        //     adjoint x/y temporaries of plane L.
+        //     x-type tiles [f][r][c]: x = x0-4+c, y = y0+r; y-type: x = x0+c, y = y0-4+r
+        auto xt_at = [&](int r, int c) {
+            const bool in = (x0 - 4 + c >= L.ixbeg) && (x0 - 4 + c <= L.ixend);
+            const float irv = A[A_IR * IH * IW + (r + 4) * IW + c];
 #pragma unroll
-            for (int i = 1; i <= 4; ++i) acc += c1(i) * (Pf[(r + 8) * PW + c + 3 + i] - Pf[(r + 8) * PW + c + 4 - i]);
-            acc *= a.hx;
-            const int gx = x0 - 4 + c;
-            const float v = acc * A[A_IR * IH * IW + (r + 4) * IW + c];
-            fdx[e] = (gx >= L.ixbeg && gx <= L.ixend) ? v : 0.0f;
-            if (f == 0) {
-                const int k = (r + 4) * IW + c;
-                const float2 t2 = img_adj(A, k, TTI ? A[A_RX * IH * IW + k] : 0.0f);
-                axs[e] = t2.x;
-                axs[TY * IW + e] = t2.y;
-            }
-        }
-        for (int e = tid; e < 2 * IH * TX; e += NT) {
-            const int f = e / (IH * TX), r = (e / TX) % IH, c = e % TX;  // y = y0-4+r, x = x0+c
-            const float* Pf = f ? P2 : P1;
-            float acc = 0.0f;
+            for (int f = 0; f < 2; ++f) {
+                const float* Pr = (f ? P2 : P1) + (r + 8) * PW + c + 4;
+                float acc = 0.0f;
 #pragma unroll
-            for (int i = 1; i <= 4; ++i)
-                acc += c1(i) * (Pf[(r + 3 + i) * PW + c + 8] - Pf[(r + 4 - i) * PW + c + 8]);
-            acc *= a.hy;
-            const int gy = y0 - 4 + r;
-            const float v = acc * A[A_IR * IH * IW + r * IW + c + 4];
-            fdy[e] = (gy >= L.iybeg && gy <= L.iyend) ? v : 0.0f;
-            if (f == 0) {
-                const int k = r * IW + c + 4;
-                const float2 t2 = img_adj(A, k, TTI ? A[A_RY * IH * IW + k] : 0.0f);
-                ays[e] = t2.x;
-                ays[IH * TX + e] = t2.y;
+                for (int i = 1; i <= 4; ++i) acc += c1(i) * (Pr[i - 1] - Pr[-i]);
+                acc *= a.hx;
+                fdx[f * TY * IW + r * IW + c] = in ? acc * irv : 0.0f;
             }
-        }
+            const int k = (r + 4) * IW + c;
+            const float2 t2 = img_adj(A, k, TTI ? A[A_RX * IH * IW + k] : 0.0f);
+            axs[r * IW + c] = t2.x;
+            axs[TY * IW + r * IW + c] = t2.y;
+        };
+        auto yt_at = [&](int r, int c) {
+            const bool in = (y0 - 4 + r >= L.iybeg) && (y0 - 4 + r <= L.iyend);
+            const float irv = A[A_IR * IH * IW + r * IW + c + 4];
+#pragma unroll
+            for (int f = 0; f < 2; ++f) {
+                const float* Pc = (f ? P2 : P1) + (r + 4) * PW + c + 8;
+                float acc = 0.0f;
+#pragma unroll
+                for (int i = 1; i <= 4; ++i) acc += c1(i) * (Pc[(i - 1) * PW] - Pc[-i * PW]);
+                acc *= a.hy;
+                fdy[f * IH * TX + r * TX + c] = in ? acc * irv : 0.0f;
+            }
+            const int k = r * IW + c + 4;
+            const float2 t2 = img_adj(A, k, TTI ? A[A_RY * IH * IW + k] : 0.0f);
+            ays[r * TX + c] = t2.x;
+            ays[IH * TX + r * TX + c] = t2.y;
+        };
+        xt_at(ty, tx);
+        if (tx < IW - TX) xt_at(ty, tx + TX);
+        yt_at(ty, tx);
+        if (ty < IH - TY) yt_at(ty + TY, tx);
         // (2) column values: z temporaries, buoyancy, D- z stage of the stored p/q
         {
             const int64_t gc = L.idx(min(x, L.ldimx - 1), min(y, L.ldimy - 1), min(max(Lz, 0), L.ldimz - 1));
@@ -1116,6 +1156,10 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             const int64_t d = ((int64_t)(z - L.izbeg) * ny + (y - L.iybeg)) * nx + (x - L.ixbeg);
             a.grho[d] += -irq[0] * rhs;
         }
+        if (++s == IMG_NSTAGE) {
+            s = 0;
+            phase ^= 1u;
+        }
     }
 }
 
@@ -1212,12 +1256,31 @@ bool layout_supported(const Layout& L)
 
 int pick_bz(const Layout& L)
 {
-    // Enough CTAs to fill the 148 SMs at one CTA per SM; longer chunks
-    // amortise the 14-plane pipeline fill.
-    const int tiles = ((L.nx() + TX - 1) / TX) * ((L.ny() + TY - 1) / TY);
-    int bz = L.nz();
-    while (bz > 32 && (long)tiles * ((L.nz() + bz - 1) / bz) < 2 * 148) bz = (bz + 1) / 2;
-    return bz;
+    // One CTA per SM (shared memory bound).  Time ~ waves * (bz + 2*LAG):
+    // fewer, longer chunks amortise the 14-plane pipeline fill, more chunks
+    // fill the 148 SMs.
+    int sms = 148;
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaGetLastError();
+    }
+    const long tiles = (long)((L.nx() + TX - 1) / TX) * ((L.ny() + TY - 1) / TY);
+    const int nz = L.nz();
+    int best = nz;
+    double best_cost = 1e300;
+    for (int nch = 1; nch <= nz; ++nch) {
+        const int bz = (nz + nch - 1) / nch;
+        if (bz < 8 && nch > 1) break;
+        const long ctas = tiles * ((nz + bz - 1) / bz);
+        const double waves = (double)((ctas + sms - 1) / sms);
+        const double cost = waves * (bz + 2 * LAG);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = bz;
+        }
+    }
+    return best;
 }
 
 } // namespace
