@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--per-kernel", action="store_true", help="reference kernel sequence instead of fused")
+    ap.add_argument("--snap-precision", choices=["fp32", "fp16", "bf16"], default="fp32",
+                    help="snapshot storage (the stencils and time update stay FP32)")
     return ap.parse_args()
 
 
@@ -221,7 +223,8 @@ def run_ours(args):
     model, true, dt, w, src, rec, desc = workload(args, rank)
     n = args.n
     cfg = P.Config(nx=n, ny=n, nz=n, dx=10.0, dy=10.0, dz=10.0, dt=dt, nt=args.nt, xcorr_step=args.xcorr,
-                   sponge_width=24, free_surface=True, fused=not args.per_kernel, save_snapshots=True)
+                   sponge_width=24, free_surface=True, fused=not args.per_kernel, save_snapshots=True,
+                   snap_precision=args.snap_precision)
     sim = P.Simulator(cfg)
     sim.set_source(*src, w)
     sim.set_receivers(rec)
@@ -335,7 +338,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, see config)",
         "config": {**desc, "parallelism": f"shot-parallel x{ws}" if ws > 1 else "single GPU",
-                   "path": "reference kernel sequence" if args.per_kernel else "fused step kernels"},
+                   "path": "reference kernel sequence" if args.per_kernel else "fused step kernels",
+                   "snapshots": args.snap_precision},
         "roofline": roofline, "hbm_frac_alg_134B": hbm_frac,
         "shots_per_hour": 3600.0 * 1e3 / ms_per_step * ws,
         "passes_ms_per_shot": passes, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,

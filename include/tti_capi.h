@@ -39,7 +39,8 @@ enum {
     TTI_ENOMEM = 2,   /* device or pinned-host allocation failed */
     TTI_ELAUNCH = 3,  /* kernel launch or CUDA runtime error */
     TTI_ETIMEOUT = 4, /* a bounded wait gave up */
-    TTI_ESTATE = 5    /* call out of order (e.g. read before any write) */
+    TTI_ESTATE = 5,   /* call out of order (e.g. read before any write) */
+    TTI_ERANGE = 6    /* a reduced-precision snapshot value saturated (results produced) */
 };
 
 typedef void* tti_stream_t;
@@ -181,6 +182,8 @@ typedef struct {
     int free_surface;     /* 1: free surface at the top interior plane (reference behaviour) */
     int fused;            /* 1: fused step kernels; 0: the reference's kernel sequence */
     int save_snapshots;   /* 1: keep the forward snapshots on the device for the adjoint */
+    int snap_precision;   /* snapshot storage: 0 FP32, 1 FP16, 2 BF16 (value * per-field power-of-two
+                             scale; needs fused = 1 and nx a multiple of 8) */
 } tti_sim_config;
 
 int tti_sim_create(const tti_sim_config* cfg, tti_sim** out);

@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtti_b200.so")
 RADIUS = 4
 
-OK, EINVAL, ENOMEM, ELAUNCH, ETIMEOUT, ESTATE = range(6)
+OK, EINVAL, ENOMEM, ELAUNCH, ETIMEOUT, ESTATE, ERANGE = range(7)
 
 
 class TTIError(RuntimeError):
@@ -56,7 +56,7 @@ class SimConfig(C.Structure):
         ("nx", I), ("ny", I), ("nz", I),
         ("dx", D), ("dy", D), ("dz", D),
         ("dt", F), ("nt", I), ("xcorr_step", I), ("sponge_width", I),
-        ("free_surface", I), ("fused", I), ("save_snapshots", I),
+        ("free_surface", I), ("fused", I), ("save_snapshots", I), ("snap_precision", I),
     ]
 
 
@@ -268,11 +268,13 @@ class Config:
     free_surface: bool = True
     fused: bool = True
     save_snapshots: bool = True
+    snap_precision: str = "fp32"  # "fp32" | "fp16" | "bf16"
 
     def c_struct(self) -> SimConfig:
+        prec = {"fp32": 0, "fp16": 1, "bf16": 2}[self.snap_precision]
         return SimConfig(self.nx, self.ny, self.nz, self.dx, self.dy, self.dz, self.dt, self.nt,
                          self.xcorr_step, self.sponge_width, int(self.free_surface), int(self.fused),
-                         int(self.save_snapshots))
+                         int(self.save_snapshots), prec)
 
 
 VOLUMES = ("field1", "field2", "field3", "field4", "irho", "model1", "model2", "model3", "model4",

@@ -7,6 +7,8 @@
 // ldimx is padded to a multiple of 32 floats (128 bytes).
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -53,6 +55,31 @@ struct Layout {
     __host__ __device__ int ny() const { return iyend - iybeg + 1; }
     __host__ __device__ int nz() const { return izend - izbeg + 1; }
 };
+
+// Snapshot storage precision: FP32, or FP16/BF16 holding value*scale with a
+// per-snapshot, per-field power-of-two scale.
+enum SnapPrec { SNAP_F32 = 0, SNAP_F16 = 1, SNAP_BF16 = 2 };
+inline size_t snap_elt_bytes(int prec) { return prec == SNAP_F32 ? 4 : 2; }
+
+// Store v (already scaled) at element i; returns true if it had to saturate.
+__device__ __forceinline__ bool snap_store(void* base, int64_t i, float v, int prec)
+{
+    if (prec == SNAP_F32) {
+        static_cast<float*>(base)[i] = v;
+        return false;
+    }
+    if (prec == SNAP_F16) {
+        const bool sat = fabsf(v) > 65504.0f;
+        static_cast<__half*>(base)[i] = __float2half_rn(fminf(fmaxf(v, -65504.0f), 65504.0f));
+        return sat;
+    }
+    static_cast<__nv_bfloat16*>(base)[i] = __float2bfloat16_rn(v);
+    return false;
+}
+template <typename T> __device__ __forceinline__ float to_f32(T v);
+template <> __device__ __forceinline__ float to_f32<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f32<__half>(__half v) { return __half2float(v); }
+template <> __device__ __forceinline__ float to_f32<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
 
 // Host-side check of a launcher's index ranges against the radius-4 halo
 // contract.  ldimz is not part of the reference launcher signatures, so the

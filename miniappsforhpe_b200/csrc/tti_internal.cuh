@@ -43,7 +43,10 @@ struct FwdStepArgs {
     const float2 *abx, *aby, *abz;
     int64_t src_index;  // -1: no source
     float src_term;     // w[n]*dt
-    float* snap;        // nullptr or 4 interior volumes: pdot, qdot, p, q
+    void* snap;                 // nullptr or 4 interior volumes: pdot, qdot, p, q
+    int snap_prec;              // SnapPrec of the store
+    const float* snap_scale;    // 4 multipliers applied before storing (reduced precision)
+    unsigned int* snap_amax;    // 4 running max |value| (float bits) of this snapshot
     int free_surface;
     int vti;            // 1: rx=ry=0, rz=1 are not read
     float dt;
@@ -79,7 +82,9 @@ struct ImageArgs {
     const float* adj2;
     const float* adj3;
     const float* adj4;
-    const float* store;
+    const void* store;
+    int snap_prec;
+    const float* snap_scale;  // 4 multipliers the slot was stored with
     int nsnap;
     int slot;
     Model m;

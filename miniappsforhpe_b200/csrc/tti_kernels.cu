@@ -583,6 +583,7 @@ const char* tti_status_string(int status)
     case TTI_ELAUNCH: return "kernel launch or CUDA error";
     case TTI_ETIMEOUT: return "timed out";
     case TTI_ESTATE: return "call out of order";
+    case TTI_ERANGE: return "reduced-precision snapshot saturated";
     default: return "unknown status";
     }
 }

@@ -115,6 +115,25 @@ __global__ void k_inject_residual(float* __restrict__ f3, float* __restrict__ f4
     f4[i] += (-1.0f / 3.0f) * v;
 }
 
+// Per-field power-of-two scale of the next reduced-precision snapshot from
+// the running max |value| of the previous one: max*scale ~ 2^11, leaving a
+// factor 32 of growth before FP16 saturates; the running max is reset.
+__global__ void k_snap_scale(float* __restrict__ scale, unsigned int* __restrict__ amax)
+{
+    const int f = threadIdx.x;
+    if (f >= 4) return;
+    const float m = __uint_as_float(amax[f]);
+    float sc = 1.0f;
+    if (m > 0.0f && isfinite(m)) {
+        int e = 0;
+        frexpf(m, &e);  // m = g * 2^e, g in [0.5, 1)
+        e = max(-100, min(100, 11 - e));
+        sc = ldexpf(1.0f, e);
+    }
+    scale[f] = sc;
+    amax[f] = 0u;
+}
+
 // Interior-only Vp image scaling g *= -2*dt_xcorr/vp (kernel_type2_small.cu:61-74).
 __global__ void k_finalize_dense(float* __restrict__ g, const float* __restrict__ m3, Layout L, float dt_xcorr)
 {
@@ -150,7 +169,9 @@ struct tti_sim {
     float2 *abx = nullptr, *aby = nullptr, *abz = nullptr;
     float4* base = nullptr;
     float *snp = nullptr, *snq = nullptr;  // halo'd p/q restored from a snapshot
-    float* snaps = nullptr;                // nsnap slots of 4 interior volumes
+    void* snaps = nullptr;                 // nsnap slots of 4 interior volumes
+    float* snap_scale = nullptr;           // nsnap x 4 storage multipliers
+    unsigned int* snap_amax = nullptr;     // 4 running max |value| (float bits)
     int nsnap = 0;
     float *grad_vp = nullptr, *grad_rho = nullptr;
     int64_t src_index = -1;
@@ -399,7 +420,8 @@ int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
     if (!cfg || !out) return TTI_EINVAL;
     *out = nullptr;
     const tti_sim_config& c = *cfg;
-    if (c.nx < 1 || c.ny < 1 || c.nz < 1 || c.nt < 1 || c.xcorr_step < 1 || !(c.dx > 0) || !(c.dy > 0) ||
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1 || c.nt < 1 || c.xcorr_step < 1 || c.snap_precision < 0 ||
+        c.snap_precision > 2 || (c.snap_precision != 0 && (!c.fused || c.nx % 8 != 0)) || !(c.dx > 0) || !(c.dy > 0) ||
         !(c.dz > 0) || !(c.dt > 0) || c.sponge_width < 0 || (c.nz <= kRadius && c.free_surface))
         return TTI_EINVAL;
     tti_sim* s = new (std::nothrow) tti_sim();
@@ -435,7 +457,11 @@ int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
     if (!rc) rc = s->alloc((void**)&s->abz, L.ldimz * sizeof(float2));
     if (!rc && c.save_snapshots) {
         s->nsnap = (c.nt - 1) / c.xcorr_step + 1;
-        rc = s->alloc((void**)&s->snaps, (size_t)s->nsnap * 4 * s->ninterior * sizeof(float));
+        rc = s->alloc((void**)&s->snaps, (size_t)s->nsnap * 4 * s->ninterior * snap_elt_bytes(c.snap_precision));
+        if (!rc) rc = s->alloc((void**)&s->snap_scale, (size_t)s->nsnap * 4 * sizeof(float));
+        if (!rc) rc = s->alloc((void**)&s->snap_amax, 4 * sizeof(unsigned int));
+        if (!rc && cudaMemsetAsync(s->snap_amax, 0, 4 * sizeof(unsigned int), s->stream) != cudaSuccess)
+            rc = cuda_rc(cudaGetLastError());
     }
     if (!rc) {
         for (float** v : vols) rc = rc ? rc : sim_zero(s, *v, s->nvol());
@@ -599,11 +625,14 @@ int tti_sim_forward(tti_sim* s, float* traces, int traces_on_device)
     }
     for (int n = 0; n < c.nt; ++n) {
         const bool snap = c.save_snapshots && (n % c.xcorr_step == 0);
-        float* slot = snap ? s->snaps + (size_t)(n / c.xcorr_step) * 4 * s->ninterior : nullptr;
+        const size_t elt = snap_elt_bytes(c.snap_precision);
+        void* slot = snap ? static_cast<unsigned char*>(s->snaps) + (size_t)(n / c.xcorr_step) * 4 * s->ninterior * elt
+                          : nullptr;
         if (!fused) {
             if ((rc = forward_per_kernel_step(s, n, st))) return rc;
             if (snap) {
-                k_snapshot_save<<<s->dense_grid(), 128, 0, st>>>(slot, s->f3, s->f4, s->f1, s->f2, L);
+                k_snapshot_save<<<s->dense_grid(), 128, 0, st>>>(static_cast<float*>(slot), s->f3, s->f4, s->f1,
+                                                                 s->f2, L);
                 s->launches++;
             }
             if (s->nrec) {
@@ -631,6 +660,14 @@ int tti_sim_forward(tti_sim* s, float* traces, int traces_on_device)
             a.src_index = s->src_index;
             a.src_term = s->src_index >= 0 ? s->wavelet[n] * c.dt : 0.0f;
             a.snap = slot;
+            a.snap_prec = c.snap_precision;
+            if (snap && c.snap_precision != SNAP_F32) {
+                float* sc = s->snap_scale + (size_t)(n / c.xcorr_step) * 4;
+                k_snap_scale<<<1, 32, 0, st>>>(sc, s->snap_amax);
+                s->launches++;
+                a.snap_scale = sc;
+                a.snap_amax = s->snap_amax;
+            }
             a.free_surface = c.free_surface;
             a.vti = s->vti ? 1 : 0;
             a.dt = c.dt;
@@ -735,15 +772,18 @@ static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device
             swap_pq(s);
         }
         if (n % c.xcorr_step == 0) {
-            const float* slot = s->snaps + (size_t)(n / c.xcorr_step) * 4 * s->ninterior;
+            const float* slot =
+                static_cast<const float*>(s->snaps) + (size_t)(n / c.xcorr_step) * 4 * s->ninterior;
             mark_begin(s, 2, st);
-            if (fused && fused_image_supported(L)) {
+            if (fused && (fused_image_supported(L) || c.snap_precision != SNAP_F32)) {
                 ImageArgs ia{};
                 ia.adj1 = s->f1;
                 ia.adj2 = s->f2;
                 ia.adj3 = s->f3;
                 ia.adj4 = s->f4;
                 ia.store = s->snaps;
+                ia.snap_prec = c.snap_precision;
+                ia.snap_scale = s->snap_scale + (size_t)(n / c.xcorr_step) * 4;
                 ia.nsnap = s->nsnap;
                 ia.slot = n / c.xcorr_step;
                 ia.m = model_of(s);

@@ -85,7 +85,7 @@ def oracle_rtm(o, lay, m, ab, cfg, src, wavelet, rec, residual=None, adjoint=Tru
         row = np.zeros(nrec, o.dtype)
         o.fwd_step(g, st, m, ab, src, float(wavelet[n]), rec, row)
         traces[n] = row
-        if n % cfg.xcorr_step == 0:
+        if adjoint and n % cfg.xcorr_step == 0:
             snaps[n] = [st[k][I].copy() for k in ("f3", "f4", "f1", "f2")]
     out = {"traces": traces, "f3": st["f3"].copy(), "f4": st["f4"].copy()}
     if not adjoint:

@@ -69,3 +69,12 @@ def test_sim_config_is_validated():
     assert e.value.status == P.EINVAL
     with pytest.raises(P.TTIError):
         P.Simulator(P.Config(nx=8, ny=8, nz=8, dt=-1.0))
+
+
+def test_reduced_precision_snapshots_need_the_fused_path():
+    with pytest.raises(P.TTIError) as e:
+        P.Simulator(P.Config(nx=48, ny=40, nz=40, nt=8, fused=False, snap_precision="fp16"))
+    assert e.value.status == P.EINVAL
+    with pytest.raises(P.TTIError) as e:  # nx not a multiple of 8
+        P.Simulator(P.Config(nx=44, ny=40, nz=40, nt=8, snap_precision="bf16"))
+    assert e.value.status == P.EINVAL
