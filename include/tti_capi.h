@@ -184,9 +184,21 @@ typedef struct {
     int save_snapshots;   /* 1: keep the forward snapshots on the device for the adjoint */
     int snap_precision;   /* snapshot storage: 0 FP32, 1 FP16, 2 BF16 (value * per-field power-of-two
                              scale; needs fused = 1 and nx a multiple of 8) */
+    int checkpoint_every; /* 0: keep every snapshot of the shot.  K > 0 (a multiple of xcorr_step;
+                             fused = 1, save_snapshots = 1): keep FP32 checkpoints of the forward
+                             state every K steps and the snapshots of one K-step segment; the
+                             adjoint recomputes each segment's snapshots from its checkpoint.
+                             Results are identical to K = 0. */
+    int use_graphs;       /* 1: each time loop (or checkpoint segment) is captured into a CUDA graph
+                             and launched as one; the instantiated graph is reused across calls */
 } tti_sim_config;
 
 int tti_sim_create(const tti_sim_config* cfg, tti_sim** out);
+
+/* Device bytes a simulator with this configuration allocates at creation
+ * (receiver buffers, nt*nrec*8 bytes + nrec*8, come on top at
+ * tti_sim_set_receivers).  Used for admission by HBM footprint. */
+int tti_sim_footprint_bytes(const tti_sim_config* cfg, int64_t* bytes);
 int tti_sim_destroy(tti_sim* sim);
 
 /* Model from host arrays over the interior (nx*ny*nz, x fastest): vp, eps,

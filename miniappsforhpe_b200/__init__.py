@@ -57,6 +57,7 @@ class SimConfig(C.Structure):
         ("dx", D), ("dy", D), ("dz", D),
         ("dt", F), ("nt", I), ("xcorr_step", I), ("sponge_width", I),
         ("free_surface", I), ("fused", I), ("save_snapshots", I), ("snap_precision", I),
+        ("checkpoint_every", I), ("use_graphs", I),
     ]
 
 
@@ -74,6 +75,7 @@ _SIGS = {
     "tti_launch_init_cijs": [V] * 13 + [L64, V],
     "tti_launch_compute_pressure": [V, V, V, L64, V],
     "tti_sim_create": [C.POINTER(SimConfig), C.POINTER(V)],
+    "tti_sim_footprint_bytes": [C.POINTER(SimConfig), C.POINTER(L64)],
     "tti_sim_destroy": [V],
     "tti_sim_set_model": [V] * 8,
     "tti_sim_set_source": [V, I, I, I, V, I],
@@ -269,12 +271,23 @@ class Config:
     fused: bool = True
     save_snapshots: bool = True
     snap_precision: str = "fp32"  # "fp32" | "fp16" | "bf16"
+    checkpoint_every: int = 0  # >0: FP32 checkpoints every K steps, snapshots recomputed per segment
+    use_graphs: bool = False  # capture each time loop into a CUDA graph
 
     def c_struct(self) -> SimConfig:
         prec = {"fp32": 0, "fp16": 1, "bf16": 2}[self.snap_precision]
         return SimConfig(self.nx, self.ny, self.nz, self.dx, self.dy, self.dz, self.dt, self.nt,
                          self.xcorr_step, self.sponge_width, int(self.free_surface), int(self.fused),
-                         int(self.save_snapshots), prec)
+                         int(self.save_snapshots), prec, int(self.checkpoint_every), int(self.use_graphs))
+
+    def footprint_bytes(self) -> int:
+        """Device bytes ``tti_sim_create`` allocates for this configuration."""
+        c = self.c_struct()
+        out = L64()
+        rc = lib().tti_sim_footprint_bytes(C.byref(c), C.byref(out))
+        if rc != OK:
+            raise TTIError(rc, "tti_sim_footprint_bytes")
+        return out.value
 
 
 VOLUMES = ("field1", "field2", "field3", "field4", "irho", "model1", "model2", "model3", "model4",

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -210,6 +211,7 @@ __global__ void __launch_bounds__(NT, 1)
         for (int c = 0; c < 4; ++c) mq[j][c] = 0.0f;
 
     const int vc = (tx + 8), vr = (ty + 8);  // this column inside a p/q tile
+    unsigned tmax[4] = {0u, 0u, 0u, 0u};    // max |stored value| seen by this thread
 
     int s = 0;           // ring slot of plane t
     uint32_t phase = 0;  // mbarrier parity of slot s for this use
@@ -451,14 +453,10 @@ __global__ void __launch_bounds__(NT, 1)
                     a.qout[gm] = -nq;
                 }
             }
-            // running max |value| of each stored field, for the next snapshot's scale
-            if (a.snap && a.snap_prec != SNAP_F32) {
+            // running max |value| of each stored field (the bits of a
+            // non-negative float order like the float)
 #pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(snapv[f])));
-                    if ((tid & 31) == 0) atomicMax(a.snap_amax + f, m);
-                }
-            }
+            for (int f = 0; f < 4; ++f) tmax[f] = max(tmax[f], __float_as_uint(fabsf(snapv[f])));
         }
         if constexpr (TTI) {
 #pragma unroll
@@ -471,6 +469,15 @@ __global__ void __launch_bounds__(NT, 1)
         if (++s == FWD_NS) {
             s = 0;
             phase ^= 1u;
+        }
+    }
+    // one atomic per warp and field for the whole z chunk; the next
+    // snapshot's scale is taken from this running max
+    if (a.snap && a.snap_prec != SNAP_F32) {
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            const unsigned m = __reduce_max_sync(0xffffffffu, tmax[f]);
+            if ((tid & 31) == 0 && m) atomicMax(a.snap_amax + f, m);
         }
     }
 }
@@ -1305,6 +1312,50 @@ int* err_word()
     return p;
 }
 
+// Kernel attributes (dynamic shared memory above 48 KB) and the error word are
+// set up once per device, outside any stream capture.
+template <typename K>
+bool set_smem(K kernel, size_t bytes)
+{
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
+}
+
+bool prepare_device()
+{
+    bool ok = err_word() != nullptr;
+    ok = ok && set_smem(k_fused_forward<false>, FWD_SMEM) && set_smem(k_fused_forward<true>, FWD_SMEM);
+    ok = ok && set_smem(k_fused_adjoint<false>, ADJ_SMEM) && set_smem(k_fused_adjoint<true>, ADJ_SMEM);
+    ok = ok && set_smem(k_fused_image<false, float>, img_smem(4)) && set_smem(k_fused_image<true, float>, img_smem(4));
+    ok = ok && set_smem(k_fused_image<false, __half>, img_smem(2)) &&
+         set_smem(k_fused_image<true, __half>, img_smem(2));
+    ok = ok && set_smem(k_fused_image<false, __nv_bfloat16>, img_smem(2)) &&
+         set_smem(k_fused_image<true, __nv_bfloat16>, img_smem(2));
+    if (!ok) cudaGetLastError();
+    return ok;
+}
+
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_prepared[kMaxDevices];  // 0 no, 1 yes, -1 failed
+std::mutex g_prepare_mu;
+
+bool kernels_prepared()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return false;
+    }
+    int v = g_prepared[dev].load(std::memory_order_acquire);
+    if (v) return v > 0;
+    std::lock_guard<std::mutex> lk(g_prepare_mu);
+    v = g_prepared[dev].load(std::memory_order_relaxed);
+    if (!v) {
+        v = prepare_device() ? 1 : -1;
+        g_prepared[dev].store(v, std::memory_order_release);
+    }
+    return v > 0;
+}
+
 bool layout_supported(const Layout& L)
 {
     // TMA box origins x0-8 and x0-4 must be multiples of 4 floats (16 bytes):
@@ -1387,20 +1438,11 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.err = err_word();
     if (!a.err) return TTI_ENOMEM;
     dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
-    static bool attr_set[2] = {false, false};
-    if (s.vti) {
-        if (!attr_set[0]) {
-            cudaFuncSetAttribute(k_fused_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM);
-            attr_set[0] = true;
-        }
+    if (!kernels_prepared()) return TTI_ELAUNCH;
+    if (s.vti)
         k_fused_forward<false><<<grid, dim3(TX, TY), FWD_SMEM, st>>>(mp, mq, mi, a);
-    } else {
-        if (!attr_set[1]) {
-            cudaFuncSetAttribute(k_fused_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM);
-            attr_set[1] = true;
-        }
+    else
         k_fused_forward<true><<<grid, dim3(TX, TY), FWD_SMEM, st>>>(mp, mq, mi, a);
-    }
     return launch_status();
 }
 
@@ -1437,20 +1479,11 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     if (!a.err) return TTI_ENOMEM;
     const bool tti = !s.vti;
     dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
-    static bool attr_set[2] = {false, false};
-    if (!tti) {
-        if (!attr_set[0]) {
-            cudaFuncSetAttribute(k_fused_adjoint<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
-            attr_set[0] = true;
-        }
+    if (!kernels_prepared()) return TTI_ELAUNCH;
+    if (!tti)
         k_fused_adjoint<false><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
-    } else {
-        if (!attr_set[1]) {
-            cudaFuncSetAttribute(k_fused_adjoint<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
-            attr_set[1] = true;
-        }
+    else
         k_fused_adjoint<true><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
-    }
     return launch_status();
 }
 
@@ -1477,12 +1510,7 @@ bool make_store_map(CUtensorMap* m, const void* base, int prec, int nx, int ny, 
 template <bool TTI, typename T>
 int launch_image_t(const ImgMaps& tm, const ImgParams& a, dim3 grid, cudaStream_t st)
 {
-    static bool attr_set = false;
     const size_t smem = img_smem(sizeof(T));
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_fused_image<TTI, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
     k_fused_image<TTI, T><<<grid, dim3(TX, TY), smem, st>>>(tm, a);
     return launch_status();
 }
@@ -1496,19 +1524,20 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     if (s.snap_prec != SNAP_F32 && !s.snap_scale) return TTI_EINVAL;
     ImgMaps tm;
     {
+        // store maps keyed by (store address, grid, slots, precision)
         static std::mutex mu;
-        static const void* cached_base = nullptr;
-        static int cached_dims[5] = {0, 0, 0, 0, -1};
-        static CUtensorMap cached;
+        static std::map<std::tuple<const void*, int, int, int, int, int>, CUtensorMap> cache;
         std::lock_guard<std::mutex> lk(mu);
-        const int dims[5] = {L.nx(), L.ny(), L.nz(), 4 * s.nsnap, s.snap_prec};
-        if (cached_base != s.store || std::memcmp(dims, cached_dims, sizeof(dims)) != 0) {
-            if (!make_store_map(&cached, s.store, s.snap_prec, L.nx(), L.ny(), L.nz(), 4 * s.nsnap, PW, PH))
+        const auto key = std::make_tuple(s.store, L.nx(), L.ny(), L.nz(), 4 * s.nsnap, s.snap_prec);
+        auto it = cache.find(key);
+        if (it == cache.end()) {
+            CUtensorMap m;
+            if (!make_store_map(&m, s.store, s.snap_prec, L.nx(), L.ny(), L.nz(), 4 * s.nsnap, PW, PH))
                 return TTI_ELAUNCH;
-            cached_base = s.store;
-            std::memcpy(cached_dims, dims, sizeof(dims));
+            if (cache.size() > 1024) cache.clear();
+            it = cache.emplace(key, m).first;
         }
-        tm.snap = cached;
+        tm.snap = it->second;
     }
     const float* arr[IMG_NADJ] = {s.adj1, s.adj2, s.m.m1, s.m.m2, s.m.m3, s.m.m4, s.m.irho, s.m.rx, s.m.ry};
     for (int k = 0; k < IMG_NADJ; ++k)
@@ -1536,6 +1565,7 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     if (!a.err) return TTI_ENOMEM;
     dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
     const bool tti = !s.vti;
+    if (!kernels_prepared()) return TTI_ELAUNCH;
     switch (s.snap_prec) {
     case SNAP_F32: return tti ? launch_image_t<true, float>(tm, a, grid, st) : launch_image_t<false, float>(tm, a, grid, st);
     case SNAP_F16: return tti ? launch_image_t<true, __half>(tm, a, grid, st) : launch_image_t<false, __half>(tm, a, grid, st);
@@ -1545,6 +1575,8 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     default: return TTI_EINVAL;
     }
 }
+
+int prepare_fused_kernels() { return kernels_prepared() ? TTI_OK : TTI_ELAUNCH; }
 
 // Bounded-wait status of the fused kernels on the current device: 0 if no
 // wait gave up since the last call; the word is cleared.

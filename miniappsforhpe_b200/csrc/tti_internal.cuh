@@ -101,4 +101,9 @@ int launch_fused_image(const Layout& L, const ImageArgs& a, cudaStream_t st);
 // (TTI_ETIMEOUT if any gave up); synchronizes the stream.
 int fused_wait_status(cudaStream_t st);
 
+// Sets the fused kernels' attributes and allocates the error word on the
+// current device (done by the first launch otherwise); call before a stream
+// capture that contains fused launches.
+int prepare_fused_kernels();
+
 } // namespace tti

@@ -156,23 +156,43 @@ inline int cuda_rc(cudaError_t e)
 
 } // namespace
 
+// Device state of one wavefield: p, q (read buffer), pdot, qdot, and the
+// second p, q buffer the fused kernels write the next step into.
+struct WaveState {
+    float *p = nullptr, *q = nullptr, *pd = nullptr, *qd = nullptr, *p2 = nullptr, *q2 = nullptr;
+    void swap()
+    {
+        std::swap(p, p2);
+        std::swap(q, q2);
+    }
+};
+
 struct tti_sim {
     tti_sim_config cfg{};
     Layout L{};
     cudaStream_t stream = nullptr;
     std::vector<void*> allocs;
-    float *f1 = nullptr, *f2 = nullptr, *f3 = nullptr, *f4 = nullptr;
-    float *g1 = nullptr, *g2 = nullptr;  // second p/q buffers (fused steps)
+    WaveState w;   // forward wavefield, then the adjoint one
+    WaveState rw;  // forward wavefield recomputed from checkpoints
+    // reference kernel sequence only (fused = 0, or imaging on grids the fused
+    // imaging kernel does not take)
     float* d[6] = {};
     float *rhs3 = nullptr, *rhs4 = nullptr;
-    float* mv[8] = {};  // irho, m1..m4, rx, ry, rz
-    float2 *abx = nullptr, *aby = nullptr, *abz = nullptr;
     float4* base = nullptr;
     float *snp = nullptr, *snq = nullptr;  // halo'd p/q restored from a snapshot
-    void* snaps = nullptr;                 // nsnap slots of 4 interior volumes
-    float* snap_scale = nullptr;           // nsnap x 4 storage multipliers
-    unsigned int* snap_amax = nullptr;     // 4 running max |value| (float bits)
-    int nsnap = 0;
+    bool aux = false;
+    float* mv[8] = {};  // irho, m1..m4, rx, ry, rz
+    float2 *abx = nullptr, *aby = nullptr, *abz = nullptr;
+    // snapshot store: nslot slots of 4 interior volumes (pdot, qdot, p, q)
+    void* snaps = nullptr;
+    float* snap_scale = nullptr;        // nslot x 4 storage multipliers
+    unsigned int* snap_amax = nullptr;  // 4 running max |value| (float bits)
+    int nsnap = 0;                      // snapshot steps in the shot
+    int nslot = 0;                      // slots held (nsnap, or one segment with checkpoints)
+    // checkpoints: ncp FP32 states (p, q, pdot, qdot interior) every ckpt steps
+    float* ckpts = nullptr;
+    unsigned int* ckpt_amax = nullptr;  // running snapshot max at each checkpoint
+    int ckpt = 0, ncp = 0;
     float *grad_vp = nullptr, *grad_rho = nullptr;
     int64_t src_index = -1;
     std::vector<float> wavelet;
@@ -182,14 +202,16 @@ struct tti_sim {
     float* resid = nullptr;   // nt*nrec device
     float* srctr = nullptr;   // nt device: adjoint p+q at the source
     bool model_set = false, forward_done = false;
+    bool sponge_active = false;
+    bool vti = false;
     bool profiling = false;
+    bool capturing = false;
+    cudaGraphExec_t gexec[3] = {};  // cached graphs: forward, adjoint (last segment), recompute segment
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<std::pair<int, size_t>> ev_marks;  // (kind, index of start event)
     double kind_ms[3] = {0, 0, 0};
     int64_t kind_n[3] = {0, 0, 0};
-    bool sponge_active = false;
-    bool vti = false;
     int64_t launches = 0;
     int64_t ninterior = 0;
 
@@ -208,14 +230,84 @@ struct tti_sim {
     }
     int64_t nvol() const { return (int64_t)L.ldimx * L.ldimy * L.ldimz; }
     dim3 dense_grid() const { return dim3((L.nx() + 127) / 128, L.ny(), L.nz()); }
+    size_t slot_bytes() const { return (size_t)4 * ninterior * snap_elt_bytes(cfg.snap_precision); }
+    void* slot_ptr(int k) const { return static_cast<unsigned char*>(snaps) + (size_t)k * slot_bytes(); }
 };
 
 namespace {
 
-int sim_zero(tti_sim* s, float* p, int64_t n)
+Layout layout_of(const tti_sim_config& c)
 {
-    if (cudaMemsetAsync(p, 0, n * sizeof(float), s->stream) != cudaSuccess) return cuda_rc(cudaGetLastError());
+    Layout L{};
+    L.ldimx = 32 * ((c.nx + 2 * kRadius - 1) / 32 + 1);
+    L.ldimy = c.ny + 2 * kRadius;
+    L.ldimz = c.nz + 2 * kRadius;
+    L.ixbeg = L.iybeg = L.izbeg = kRadius;
+    L.ixend = kRadius + c.nx - 1;
+    L.iyend = kRadius + c.ny - 1;
+    L.izend = kRadius + c.nz - 1;
+    return L;
+}
+
+int validate(const tti_sim_config& c)
+{
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1 || c.nt < 1 || c.xcorr_step < 1 || !(c.dx > 0) || !(c.dy > 0) ||
+        !(c.dz > 0) || !(c.dt > 0) || c.sponge_width < 0 || (c.nz <= kRadius && c.free_surface))
+        return TTI_EINVAL;
+    if (c.snap_precision < 0 || c.snap_precision > 2) return TTI_EINVAL;
+    if (c.snap_precision != 0 && (!c.fused || c.nx % 8 != 0)) return TTI_EINVAL;
+    if (c.checkpoint_every < 0) return TTI_EINVAL;
+    if (c.checkpoint_every > 0 && (c.checkpoint_every % c.xcorr_step != 0 || !c.fused || !c.save_snapshots))
+        return TTI_EINVAL;
     return TTI_OK;
+}
+
+// Device memory of a simulator, by the same plan tti_sim_create allocates.
+struct Plan {
+    size_t core = 0, aux = 0, snaps = 0, ckpts = 0, recompute = 0;
+    bool need_aux = false;
+    int nsnap = 0, nslot = 0, ncp = 0;
+    size_t total() const { return core + aux + snaps + ckpts + recompute; }
+};
+
+Plan plan_of(const tti_sim_config& c)
+{
+    Plan pl;
+    const Layout L = layout_of(c);
+    const size_t vb = (size_t)L.ldimx * L.ldimy * L.ldimz * sizeof(float);
+    const size_t nin = (size_t)c.nx * c.ny * c.nz;
+    pl.core = 6 * vb + 8 * vb + 2 * nin * sizeof(float) + (size_t)c.nt * sizeof(float) +
+              (size_t)(L.ldimx + L.ldimy + L.ldimz) * sizeof(float2);
+    pl.need_aux = !c.fused || (c.save_snapshots && !fused_image_supported(L));
+    if (pl.need_aux) pl.aux = 10 * vb + 4 * vb;  // rhs3, rhs4, snp, snq, six derivatives, 4-float scratch
+    if (c.save_snapshots) {
+        pl.nsnap = (c.nt - 1) / c.xcorr_step + 1;
+        pl.nslot = pl.nsnap;
+        if (c.checkpoint_every > 0) {
+            pl.ncp = (c.nt - 1) / c.checkpoint_every + 1;
+            pl.nslot = c.checkpoint_every / c.xcorr_step;
+            pl.ckpts = (size_t)pl.ncp * 4 * nin * sizeof(float) + (size_t)pl.ncp * 4 * sizeof(unsigned int);
+            pl.recompute = 6 * vb;
+        }
+        pl.snaps = (size_t)pl.nslot * 4 * nin * snap_elt_bytes(c.snap_precision) + (size_t)pl.nslot * 4 * sizeof(float) +
+                   4 * sizeof(unsigned int);
+    }
+    return pl;
+}
+
+int sim_zero(tti_sim* s, void* p, size_t bytes)
+{
+    if (cudaMemsetAsync(p, 0, bytes, s->stream) != cudaSuccess) return cuda_rc(cudaGetLastError());
+    return TTI_OK;
+}
+
+int zero_state(tti_sim* s, WaveState& w)
+{
+    const size_t vb = (size_t)s->nvol() * sizeof(float);
+    int rc = TTI_OK;
+    for (float* v : {w.p, w.q, w.pd, w.qd, w.p2, w.q2})
+        if (!rc && v) rc = sim_zero(s, v, vb);
+    return rc;
 }
 
 // Sponge profile: damping factor G(k) = exp(-(0.3*(W-k)/W)^2) on the k-th cell
@@ -233,26 +325,75 @@ std::vector<float2> sponge_axis(int n, int ldim, int width, bool absorb_low)
     return ab;
 }
 
+Model model_of(tti_sim* s) { return Model{s->mv[0], s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->mv[5], s->mv[6], s->mv[7]}; }
+
+// ---------------------------------------------------------------------------
+// Optional per-launch timing of the step kernels (CUDA events on the
+// simulator's stream): kind 0 = forward step, 1 = adjoint step, 2 = imaging.
+cudaEvent_t next_event(tti_sim* s)
+{
+    if (s->ev_used == s->ev_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        s->ev_pool.push_back(e);
+    }
+    return s->ev_pool[s->ev_used++];
+}
+void mark_begin(tti_sim* s, int kind, cudaStream_t st)
+{
+    if (!s->profiling || s->capturing) return;
+    size_t k = s->ev_used;
+    cudaEvent_t e = next_event(s);
+    if (!e) return;
+    cudaEventRecord(e, st);
+    s->ev_marks.push_back({kind, k});
+}
+void mark_end(tti_sim* s, cudaStream_t st)
+{
+    if (!s->profiling || s->capturing || s->ev_marks.empty()) return;
+    cudaEvent_t e = next_event(s);
+    if (e) cudaEventRecord(e, st);
+}
+void collect_marks(tti_sim* s)
+{
+    for (auto& m : s->ev_marks) {
+        if (m.second + 1 >= s->ev_used) continue;
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, s->ev_pool[m.second], s->ev_pool[m.second + 1]) == cudaSuccess) {
+            s->kind_ms[m.first] += ms;
+            s->kind_n[m.first] += 1;
+        }
+    }
+    cudaGetLastError();
+    s->ev_marks.clear();
+    s->ev_used = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Reference kernel sequence (fused = 0), on the main state in place.
 int forward_per_kernel_step(tti_sim* s, int n, cudaStream_t st)
 {
     const Layout& L = s->L;
-    int rc;
-    rc = tti_launch_kernel_loop2(s->f1, s->f2, s->f3, s->f4, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg, L.iyend,
-                                 L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby, (const float*)s->abz,
-                                 s->cfg.dt, st);
+    const tti_sim_config& c = s->cfg;
+    WaveState& w = s->w;
+    int rc = tti_launch_kernel_loop2(w.p, w.q, w.pd, w.qd, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg, L.iyend,
+                                     L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby,
+                                     (const float*)s->abz, c.dt, st);
     if (rc) return rc;
     s->launches++;
-    if (s->cfg.free_surface) {
-        if ((rc = tti_launch_kernel_loop4(s->f1, s->f2, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
+    if (c.free_surface) {
+        if ((rc = tti_launch_kernel_loop4(w.p, w.q, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
         s->launches++;
     }
-    float invdx = 1.0 / s->cfg.dx, invdy = 1.0 / s->cfg.dy, invdz = 1.0 / s->cfg.dz;
-    if ((rc = tti_launch_fwd_kernel2_drv(s->f1, s->f2, s->mv[0], s->d[0], s->d[1], s->d[2], s->d[3], s->d[4],
-                                         s->d[5], L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg, L.izend, invdx, invdy,
-                                         invdz, L.ldimx, L.ldimy, 8, st)))
+    if ((rc = tti_launch_fwd_kernel2_drv(w.p, w.q, s->mv[0], s->d[0], s->d[1], s->d[2], s->d[3], s->d[4], s->d[5],
+                                         L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg, L.izend, (float)(1.0 / c.dx),
+                                         (float)(1.0 / c.dy), (float)(1.0 / c.dz), L.ldimx, L.ldimy, 8, st)))
         return rc;
     s->launches++;
-    if (s->cfg.free_surface) {
+    if (c.free_surface) {
         if ((rc = tti_launch_kernel_loop4_derivatives(s->d[0], s->d[1], s->d[2], s->d[3], s->d[4], s->d[5], L.ldimx,
                                                       L.ldimy, L.izbeg, st)))
             return rc;
@@ -260,14 +401,14 @@ int forward_per_kernel_step(tti_sim* s, int n, cudaStream_t st)
     }
     // argument order of launch_update_rho_fwd_main_loop_2_1: dx, dx2, dy, dy2, dz, dz2
     if ((rc = tti_launch_update_rho_fwd_main_loop_2_1(
-             s->f3, s->f4, s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5], s->f1, s->f2, s->mv[0], s->mv[1],
+             w.pd, w.qd, s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5], w.p, w.q, s->mv[0], s->mv[1],
              s->mv[2], s->mv[3], s->mv[4], s->mv[5], s->mv[6], s->mv[7], nullptr, nullptr, nullptr, nullptr, nullptr,
              nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, L.ixbeg, L.ixend, L.iybeg, L.iyend,
-             L.izbeg, L.izend, L.ldimx, L.ldimy, s->cfg.dt, s->cfg.dx, s->cfg.dy, s->cfg.dz, 0, 8, 0, 0, 0, st)))
+             L.izbeg, L.izend, L.ldimx, L.ldimy, c.dt, c.dx, c.dy, c.dz, 0, 8, 0, 0, 0, st)))
         return rc;
     s->launches++;
     if (s->src_index >= 0) {
-        k_add_source<<<1, 1, 0, st>>>(s->f3, s->f4, s->src_index, s->wavelet[n] * s->cfg.dt);
+        k_add_source<<<1, 1, 0, st>>>(w.pd, w.qd, s->src_index, s->wavelet[n] * c.dt);
         s->launches++;
     }
     return launch_status();
@@ -277,8 +418,9 @@ int adjoint_per_kernel_step(tti_sim* s, cudaStream_t st)
 {
     const Layout& L = s->L;
     const tti_sim_config& c = s->cfg;
-    int rc = launch_base(s->f1, s->f2, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->base, L.ixbeg, L.ixend, L.iybeg,
-                         L.iyend, L.izbeg, L.izend, L.ldimx, L.ldimy, st);
+    WaveState& w = s->w;
+    int rc = launch_base(w.p, w.q, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->base, L.ixbeg, L.ixend, L.iybeg, L.iyend,
+                         L.izbeg, L.izend, L.ldimx, L.ldimy, st);
     if (rc) return rc;
     rc = launch_adj_drv_with_base(s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5], s->rhs3, s->rhs4, s->base,
                                   s->mv[0], s->mv[5], s->mv[6], s->mv[7], L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg,
@@ -293,35 +435,36 @@ int adjoint_per_kernel_step(tti_sim* s, cudaStream_t st)
             return rc;
         s->launches++;
     }
-    if ((rc = tti_launch_update_adj_kernel_main_3(s->f3, s->f4, s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5],
+    if ((rc = tti_launch_update_adj_kernel_main_3(w.pd, w.qd, s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5],
                                                   s->rhs3, s->rhs4, (const float*)s->abx, (const float*)s->aby,
                                                   (const float*)s->abz, L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg,
                                                   L.izend, L.ldimx, L.ldimy, c.dt, c.dx, c.dy, c.dz, 0, 0, 0, 8,
                                                   s->sponge_active ? 1 : 0, st)))
         return rc;
     s->launches++;
-    if ((rc = tti_launch_kernel_loop2(s->f1, s->f2, s->f3, s->f4, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg,
-                                      L.iyend, L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby,
+    if ((rc = tti_launch_kernel_loop2(w.p, w.q, w.pd, w.qd, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg, L.iyend,
+                                      L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby,
                                       (const float*)s->abz, c.dt, st)))
         return rc;
     s->launches++;
     if (c.free_surface) {
-        if ((rc = tti_launch_kernel_loop4(s->f1, s->f2, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
+        if ((rc = tti_launch_kernel_loop4(w.p, w.q, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
         s->launches++;
     }
     return TTI_OK;
 }
 
-// Imaging at a snapshot step (reference order, simulator2SetUp.cu:753-781):
-// Vp image, forward derivatives of the stored p/q, derivative mirror,
-// density gradient with the current adjoint p/q.
+// Imaging at a snapshot step with the reference kernels
+// (simulator2SetUp.cu:753-781): Vp image, forward derivatives of the stored
+// p/q, derivative mirror, density gradient with the current adjoint p/q.
 int image_per_kernel(tti_sim* s, const float* slot, cudaStream_t st)
 {
     const Layout& L = s->L;
     const tti_sim_config& c = s->cfg;
+    WaveState& w = s->w;
     int64_t n = s->ninterior;
-    int rc = tti_launch_update_Vp_gradient(slot, slot + n, s->grad_vp, s->f3, s->f4, L.ixbeg, L.ixend, L.iybeg,
-                                           L.iyend, L.izbeg, L.izend, L.nx(), L.ny(), L.ldimx, L.ldimy, st);
+    int rc = tti_launch_update_Vp_gradient(slot, slot + n, s->grad_vp, w.pd, w.qd, L.ixbeg, L.ixend, L.iybeg, L.iyend,
+                                           L.izbeg, L.izend, L.nx(), L.ny(), L.ldimx, L.ldimy, st);
     if (rc) return rc;
     k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(s->snp, const_cast<float*>(slot + 2 * n), L);
     k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(s->snq, const_cast<float*>(slot + 3 * n), L);
@@ -342,7 +485,7 @@ int image_per_kernel(tti_sim* s, const float* slot, cudaStream_t st)
             return rc;
         s->launches++;
     }
-    if ((rc = launch_base(s->f1, s->f2, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->base, L.ixbeg, L.ixend, L.iybeg,
+    if ((rc = launch_base(w.p, w.q, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->base, L.ixbeg, L.ixend, L.iybeg,
                           L.iyend, L.izbeg, L.izend, L.ldimx, L.ldimy, st)))
         return rc;
     if ((rc = launch_rho_gradient_with_base(s->grad_rho, s->d[0], s->d[3], s->d[1], s->d[4], s->d[2], s->d[5],
@@ -354,101 +497,254 @@ int image_per_kernel(tti_sim* s, const float* slot, cudaStream_t st)
     return launch_status();
 }
 
-void swap_pq(tti_sim* s)
+// ---------------------------------------------------------------------------
+// Fused path.
+// p/q of step 0 (loop2 + free surface of the reference step; the fused
+// kernel of step n ends with the p/q update of step n+1).
+int fused_prologue(tti_sim* s, WaveState& w, cudaStream_t st)
 {
-    float* t = s->f1;
-    s->f1 = s->g1;
-    s->g1 = t;
-    t = s->f2;
-    s->f2 = s->g2;
-    s->g2 = t;
+    const Layout& L = s->L;
+    const tti_sim_config& c = s->cfg;
+    int rc = tti_launch_kernel_loop2(w.p, w.q, w.pd, w.qd, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg, L.iyend,
+                                     L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby,
+                                     (const float*)s->abz, c.dt, st);
+    s->launches++;
+    if (!rc && c.free_surface) {
+        rc = tti_launch_kernel_loop4(w.p, w.q, L.ldimx, L.ldimy, L.izbeg, st);
+        s->launches++;
+    }
+    return rc;
 }
 
-// Optional per-launch timing of the step kernels (CUDA events on the
-// simulator's stream): kind 0 = forward step, 1 = adjoint step, 2 = imaging.
-cudaEvent_t next_event(tti_sim* s)
+// One fused forward step n on state w; the snapshot (if any) goes to slot k.
+int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t st)
 {
-    if (s->ev_used == s->ev_pool.size()) {
-        cudaEvent_t e;
-        if (cudaEventCreate(&e) != cudaSuccess) {
+    const tti_sim_config& c = s->cfg;
+    FwdStepArgs a{};
+    a.pin = w.p;
+    a.qin = w.q;
+    a.pout = w.p2;
+    a.qout = w.q2;
+    a.f3 = w.pd;
+    a.f4 = w.qd;
+    a.m = model_of(s);
+    a.abx = s->abx;
+    a.aby = s->aby;
+    a.abz = s->abz;
+    a.src_index = s->src_index;
+    a.src_term = s->src_index >= 0 ? s->wavelet[n] * c.dt : 0.0f;
+    a.snap = slot >= 0 ? s->slot_ptr(slot) : nullptr;
+    a.snap_prec = c.snap_precision;
+    if (slot >= 0 && c.snap_precision != SNAP_F32) {
+        float* sc = s->snap_scale + (size_t)slot * 4;
+        k_snap_scale<<<1, 32, 0, st>>>(sc, s->snap_amax);
+        s->launches++;
+        a.snap_scale = sc;
+        a.snap_amax = s->snap_amax;
+    }
+    a.free_surface = c.free_surface;
+    a.vti = s->vti ? 1 : 0;
+    a.dt = c.dt;
+    a.dx = c.dx;
+    a.dy = c.dy;
+    a.dz = c.dz;
+    mark_begin(s, 0, st);
+    int rc = launch_fused_forward(s->L, a, st);
+    mark_end(s, st);
+    if (rc) return rc;
+    s->launches++;
+    w.swap();
+    return TTI_OK;
+}
+
+int fused_adjoint_step(tti_sim* s, cudaStream_t st)
+{
+    const tti_sim_config& c = s->cfg;
+    WaveState& w = s->w;
+    AdjStepArgs a{};
+    a.pin = w.p;
+    a.qin = w.q;
+    a.pout = w.p2;
+    a.qout = w.q2;
+    a.f3 = w.pd;
+    a.f4 = w.qd;
+    a.m = model_of(s);
+    a.abx = s->abx;
+    a.aby = s->aby;
+    a.abz = s->abz;
+    a.sponge_active = s->sponge_active ? 1 : 0;
+    a.free_surface = c.free_surface;
+    a.vti = s->vti ? 1 : 0;
+    a.dt = c.dt;
+    a.dx = c.dx;
+    a.dy = c.dy;
+    a.dz = c.dz;
+    mark_begin(s, 1, st);
+    int rc = launch_fused_adjoint(s->L, a, st);
+    mark_end(s, st);
+    if (rc) return rc;
+    s->launches++;
+    w.swap();
+    return TTI_OK;
+}
+
+int image_step(tti_sim* s, int slot, cudaStream_t st)
+{
+    const tti_sim_config& c = s->cfg;
+    int rc;
+    mark_begin(s, 2, st);
+    if (c.fused && (c.snap_precision != SNAP_F32 || fused_image_supported(s->L))) {
+        ImageArgs ia{};
+        ia.adj1 = s->w.p;
+        ia.adj2 = s->w.q;
+        ia.adj3 = s->w.pd;
+        ia.adj4 = s->w.qd;
+        ia.store = s->snaps;
+        ia.snap_prec = c.snap_precision;
+        ia.snap_scale = s->snap_scale + (size_t)slot * 4;
+        ia.nsnap = s->nslot;
+        ia.slot = slot;
+        ia.m = model_of(s);
+        ia.grad_vp = s->grad_vp;
+        ia.grad_rho = s->grad_rho;
+        ia.free_surface = c.free_surface;
+        ia.vti = s->vti ? 1 : 0;
+        ia.dx = c.dx;
+        ia.dy = c.dy;
+        ia.dz = c.dz;
+        rc = launch_fused_image(s->L, ia, st);
+        s->launches++;
+    } else {
+        rc = image_per_kernel(s, static_cast<const float*>(s->slot_ptr(slot)), st);
+    }
+    mark_end(s, st);
+    return rc;
+}
+
+int receivers_step(tti_sim* s, WaveState& w, int n, cudaStream_t st)
+{
+    if (!s->nrec) return TTI_OK;
+    k_receivers<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->traces + (size_t)n * s->nrec, w.p, w.q, s->rec, s->nrec);
+    s->launches++;
+    return launch_status();
+}
+
+// Checkpoint k: the state at the start of step k*ckpt (interior p, q, pdot,
+// qdot in FP32) and the running snapshot max of that moment.
+int save_checkpoint(tti_sim* s, WaveState& w, int k, cudaStream_t st)
+{
+    float* slot = s->ckpts + (size_t)k * 4 * s->ninterior;
+    k_snapshot_save<<<s->dense_grid(), 128, 0, st>>>(slot, w.p, w.q, w.pd, w.qd, s->L);
+    s->launches++;
+    if (cudaMemcpyAsync(s->ckpt_amax + 4 * k, s->snap_amax, 4 * sizeof(unsigned int), cudaMemcpyDeviceToDevice, st) !=
+        cudaSuccess)
+        return cuda_rc(cudaGetLastError());
+    return launch_status();
+}
+
+int restore_checkpoint(tti_sim* s, WaveState& w, int k, cudaStream_t st)
+{
+    const int64_t n = s->ninterior;
+    float* slot = s->ckpts + (size_t)k * 4 * n;
+    int rc = zero_state(s, w);
+    if (rc) return rc;
+    k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(w.p, slot, s->L);
+    k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(w.q, slot + n, s->L);
+    k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(w.pd, slot + 2 * n, s->L);
+    k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(w.qd, slot + 3 * n, s->L);
+    s->launches += 4;
+    if (s->cfg.free_surface) {  // the halo above the surface is the mirror of the interior
+        if ((rc = tti_launch_kernel_loop4(w.p, w.q, s->L.ldimx, s->L.ldimy, s->L.izbeg, st))) return rc;
+        s->launches++;
+    }
+    if (cudaMemcpyAsync(s->snap_amax, s->ckpt_amax + 4 * k, 4 * sizeof(unsigned int), cudaMemcpyDeviceToDevice, st) !=
+        cudaSuccess)
+        return cuda_rc(cudaGetLastError());
+    return launch_status();
+}
+
+// Run `body` either directly on the simulator's stream or captured into a
+// CUDA graph that is then launched once.  The instantiated graph of each kind
+// is kept and updated in place when the next capture has the same topology.
+template <typename F>
+int run_on_stream(tti_sim* s, int kind, F body)
+{
+    cudaStream_t st = s->stream;
+    if (!s->cfg.use_graphs) return body(st);
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_rc(cudaGetLastError());
+    s->capturing = true;
+    int rc = body(st);
+    s->capturing = false;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (!rc && e != cudaSuccess) rc = cuda_rc(e);
+    cudaGraphExec_t& ge = s->gexec[kind];
+    if (!rc && ge) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(ge, g, &info) != cudaSuccess) {
             cudaGetLastError();
-            return nullptr;
-        }
-        s->ev_pool.push_back(e);
-    }
-    return s->ev_pool[s->ev_used++];
-}
-void mark_begin(tti_sim* s, int kind, cudaStream_t st)
-{
-    if (!s->profiling) return;
-    size_t k = s->ev_used;
-    cudaEvent_t e = next_event(s);
-    if (!e) return;
-    cudaEventRecord(e, st);
-    s->ev_marks.push_back({kind, k});
-}
-void mark_end(tti_sim* s, cudaStream_t st)
-{
-    if (!s->profiling || s->ev_marks.empty()) return;
-    cudaEvent_t e = next_event(s);
-    if (e) cudaEventRecord(e, st);
-}
-// After a stream sync: fold the recorded pairs into the per-kind totals.
-void collect_marks(tti_sim* s)
-{
-    for (auto& m : s->ev_marks) {
-        if (m.second + 1 >= s->ev_used) continue;
-        float ms = 0;
-        if (cudaEventElapsedTime(&ms, s->ev_pool[m.second], s->ev_pool[m.second + 1]) == cudaSuccess) {
-            s->kind_ms[m.first] += ms;
-            s->kind_n[m.first] += 1;
+            cudaGraphExecDestroy(ge);
+            ge = nullptr;
         }
     }
+    if (!rc && !ge && cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) {
+        rc = cuda_rc(cudaGetLastError());
+        ge = nullptr;
+    }
+    if (!rc && cudaGraphLaunch(ge, st) != cudaSuccess) rc = cuda_rc(cudaGetLastError());
+    if (g) cudaGraphDestroy(g);
     cudaGetLastError();
-    s->ev_marks.clear();
-    s->ev_used = 0;
+    return rc;
 }
-
-Model model_of(tti_sim* s) { return Model{s->mv[0], s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->mv[5], s->mv[6], s->mv[7]}; }
 
 } // namespace
 
 extern "C" {
+
+int tti_sim_footprint_bytes(const tti_sim_config* cfg, int64_t* bytes)
+{
+    if (!cfg || !bytes) return TTI_EINVAL;
+    int rc = validate(*cfg);
+    if (rc) return rc;
+    *bytes = (int64_t)plan_of(*cfg).total();
+    return TTI_OK;
+}
 
 int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
 {
     if (!cfg || !out) return TTI_EINVAL;
     *out = nullptr;
     const tti_sim_config& c = *cfg;
-    if (c.nx < 1 || c.ny < 1 || c.nz < 1 || c.nt < 1 || c.xcorr_step < 1 || c.snap_precision < 0 ||
-        c.snap_precision > 2 || (c.snap_precision != 0 && (!c.fused || c.nx % 8 != 0)) || !(c.dx > 0) || !(c.dy > 0) ||
-        !(c.dz > 0) || !(c.dt > 0) || c.sponge_width < 0 || (c.nz <= kRadius && c.free_surface))
-        return TTI_EINVAL;
+    int rc = validate(c);
+    if (rc) return rc;
+    if (c.use_graphs && c.fused) {
+        // first launches set kernel attributes and allocate the error word:
+        // do that before any capture
+        if ((rc = prepare_fused_kernels())) return rc;
+    }
     tti_sim* s = new (std::nothrow) tti_sim();
     if (!s) return TTI_ENOMEM;
     s->cfg = c;
-    Layout& L = s->L;
-    L.ldimx = 32 * ((c.nx + 2 * kRadius - 1) / 32 + 1);
-    L.ldimy = c.ny + 2 * kRadius;
-    L.ldimz = c.nz + 2 * kRadius;
-    L.ixbeg = L.iybeg = L.izbeg = kRadius;
-    L.ixend = kRadius + c.nx - 1;
-    L.iyend = kRadius + c.ny - 1;
-    L.izend = kRadius + c.nz - 1;
+    s->L = layout_of(c);
+    const Layout& L = s->L;
     s->ninterior = (int64_t)c.nx * c.ny * c.nz;
-    int rc = TTI_OK;
+    const Plan pl = plan_of(c);
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         delete s;
         return TTI_ELAUNCH;
     }
-    size_t vb = (size_t)s->nvol() * sizeof(float);
-    float** vols[] = {&s->f1, &s->f2, &s->f3, &s->f4, &s->g1, &s->g2, &s->rhs3, &s->rhs4, &s->snp, &s->snq,
-                      &s->d[0], &s->d[1], &s->d[2], &s->d[3], &s->d[4], &s->d[5]};
-    for (float** v : vols)
+    const size_t vb = (size_t)s->nvol() * sizeof(float);
+    for (float** v : {&s->w.p, &s->w.q, &s->w.pd, &s->w.qd, &s->w.p2, &s->w.q2})
         if (!rc) rc = s->alloc((void**)v, vb);
     for (int k = 0; k < 8 && !rc; ++k) rc = s->alloc((void**)&s->mv[k], vb);
-    if (!rc) rc = s->alloc((void**)&s->base, (size_t)s->nvol() * sizeof(float4));
+    if (!rc && pl.need_aux) {
+        s->aux = true;
+        for (float** v : {&s->rhs3, &s->rhs4, &s->snp, &s->snq, &s->d[0], &s->d[1], &s->d[2], &s->d[3], &s->d[4],
+                          &s->d[5]})
+            if (!rc) rc = s->alloc((void**)v, vb);
+        if (!rc) rc = s->alloc((void**)&s->base, (size_t)s->nvol() * sizeof(float4));
+    }
     if (!rc) rc = s->alloc((void**)&s->grad_vp, s->ninterior * sizeof(float));
     if (!rc) rc = s->alloc((void**)&s->grad_rho, s->ninterior * sizeof(float));
     if (!rc) rc = s->alloc((void**)&s->srctr, (size_t)c.nt * sizeof(float));
@@ -456,18 +752,28 @@ int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
     if (!rc) rc = s->alloc((void**)&s->aby, L.ldimy * sizeof(float2));
     if (!rc) rc = s->alloc((void**)&s->abz, L.ldimz * sizeof(float2));
     if (!rc && c.save_snapshots) {
-        s->nsnap = (c.nt - 1) / c.xcorr_step + 1;
-        rc = s->alloc((void**)&s->snaps, (size_t)s->nsnap * 4 * s->ninterior * snap_elt_bytes(c.snap_precision));
-        if (!rc) rc = s->alloc((void**)&s->snap_scale, (size_t)s->nsnap * 4 * sizeof(float));
+        s->nsnap = pl.nsnap;
+        s->nslot = pl.nslot;
+        rc = s->alloc(&s->snaps, (size_t)s->nslot * s->slot_bytes());
+        if (!rc) rc = s->alloc((void**)&s->snap_scale, (size_t)s->nslot * 4 * sizeof(float));
         if (!rc) rc = s->alloc((void**)&s->snap_amax, 4 * sizeof(unsigned int));
-        if (!rc && cudaMemsetAsync(s->snap_amax, 0, 4 * sizeof(unsigned int), s->stream) != cudaSuccess)
-            rc = cuda_rc(cudaGetLastError());
+        if (!rc && c.checkpoint_every > 0) {
+            s->ckpt = c.checkpoint_every;
+            s->ncp = pl.ncp;
+            rc = s->alloc((void**)&s->ckpts, (size_t)s->ncp * 4 * s->ninterior * sizeof(float));
+            if (!rc) rc = s->alloc((void**)&s->ckpt_amax, (size_t)s->ncp * 4 * sizeof(unsigned int));
+            for (float** v : {&s->rw.p, &s->rw.q, &s->rw.pd, &s->rw.qd, &s->rw.p2, &s->rw.q2})
+                if (!rc) rc = s->alloc((void**)v, vb);
+        }
     }
-    if (!rc) {
-        for (float** v : vols) rc = rc ? rc : sim_zero(s, *v, s->nvol());
-        if (!rc) rc = sim_zero(s, s->grad_vp, s->ninterior);
-        if (!rc) rc = sim_zero(s, s->grad_rho, s->ninterior);
-    }
+    if (!rc) rc = zero_state(s, s->w);
+    if (!rc && s->ckpt) rc = zero_state(s, s->rw);
+    if (!rc && s->aux)
+        for (float* v : {s->rhs3, s->rhs4, s->snp, s->snq, s->d[0], s->d[1], s->d[2], s->d[3], s->d[4], s->d[5]})
+            rc = rc ? rc : sim_zero(s, v, vb);
+    if (!rc) rc = sim_zero(s, s->grad_vp, s->ninterior * sizeof(float));
+    if (!rc) rc = sim_zero(s, s->grad_rho, s->ninterior * sizeof(float));
+    if (!rc && s->snap_amax) rc = sim_zero(s, s->snap_amax, 4 * sizeof(unsigned int));
     if (!rc) {
         auto ax = sponge_axis(c.nx, L.ldimx, c.sponge_width, true);
         auto ay = sponge_axis(c.ny, L.ldimy, c.sponge_width, true);
@@ -492,6 +798,8 @@ int tti_sim_destroy(tti_sim* s)
     if (!s) return TTI_EINVAL;
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    for (cudaGraphExec_t g : s->gexec)
+        if (g) cudaGraphExecDestroy(g);
     for (void* p : s->allocs) cudaFree(p);
     if (s->stream) cudaStreamDestroy(s->stream);
     cudaGetLastError();
@@ -600,97 +908,55 @@ int tti_sim_set_receivers(tti_sim* s, int nrec, const int* ixyz)
 
 int tti_sim_forward(tti_sim* s, float* traces, int traces_on_device)
 {
-    if (!s || !s->model_set) return s ? TTI_ESTATE : TTI_EINVAL;
+    if (!s) return TTI_EINVAL;
+    if (!s->model_set) return TTI_ESTATE;
     const tti_sim_config& c = s->cfg;
-    const Layout& L = s->L;
-    cudaStream_t st = s->stream;
     s->launches = 0;
-    int rc = TTI_OK;
-    for (float* v : {s->f1, s->f2, s->f3, s->f4, s->g1, s->g2})
-        if (!rc) rc = sim_zero(s, v, s->nvol());
+    s->forward_done = false;
+    int rc = zero_state(s, s->w);
+    if (!rc && s->snap_amax) rc = sim_zero(s, s->snap_amax, 4 * sizeof(unsigned int));
     if (rc) return rc;
     const bool fused = c.fused != 0;
-    if (fused) {
-        // Step-0 p update of the reference step (loop2 + free surface); the
-        // fused kernel of step n then ends with the p update of step n+1.
-        rc = tti_launch_kernel_loop2(s->f1, s->f2, s->f3, s->f4, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg,
-                                     L.iyend, L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby,
-                                     (const float*)s->abz, c.dt, st);
-        s->launches++;
-        if (!rc && c.free_surface) {
-            rc = tti_launch_kernel_loop4(s->f1, s->f2, L.ldimx, L.ldimy, L.izbeg, st);
-            s->launches++;
+    // With checkpoints the store holds one segment: every snapshot step still
+    // writes its slot (the running max behind the FP16/BF16 scales then
+    // evolves exactly as without checkpoints), and the last segment's
+    // snapshots are the ones left for the adjoint.
+    rc = run_on_stream(s, 0, [&](cudaStream_t st) -> int {
+        int r = TTI_OK;
+        if (fused && (r = fused_prologue(s, s->w, st))) return r;
+        for (int n = 0; n < c.nt; ++n) {
+            if (s->ckpt && n % s->ckpt == 0 && (r = save_checkpoint(s, s->w, n / s->ckpt, st))) return r;
+            int slot = -1;
+            if (c.save_snapshots && n % c.xcorr_step == 0)
+                slot = s->ckpt ? (n % s->ckpt) / c.xcorr_step : n / c.xcorr_step;
+            if (!fused) {
+                if ((r = forward_per_kernel_step(s, n, st))) return r;
+                if (slot >= 0) {
+                    k_snapshot_save<<<s->dense_grid(), 128, 0, st>>>(static_cast<float*>(s->slot_ptr(slot)), s->w.pd,
+                                                                     s->w.qd, s->w.p, s->w.q, s->L);
+                    s->launches++;
+                }
+                if ((r = receivers_step(s, s->w, n, st))) return r;
+            } else {
+                if ((r = receivers_step(s, s->w, n, st))) return r;
+                if ((r = fused_forward_step(s, s->w, n, slot, st))) return r;
+            }
+            if ((r = launch_status())) return r;
         }
-        if (rc) return rc;
-    }
-    for (int n = 0; n < c.nt; ++n) {
-        const bool snap = c.save_snapshots && (n % c.xcorr_step == 0);
-        const size_t elt = snap_elt_bytes(c.snap_precision);
-        void* slot = snap ? static_cast<unsigned char*>(s->snaps) + (size_t)(n / c.xcorr_step) * 4 * s->ninterior * elt
-                          : nullptr;
-        if (!fused) {
-            if ((rc = forward_per_kernel_step(s, n, st))) return rc;
-            if (snap) {
-                k_snapshot_save<<<s->dense_grid(), 128, 0, st>>>(static_cast<float*>(slot), s->f3, s->f4, s->f1,
-                                                                 s->f2, L);
-                s->launches++;
-            }
-            if (s->nrec) {
-                k_receivers<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->traces + (size_t)n * s->nrec, s->f1, s->f2,
-                                                                  s->rec, s->nrec);
-                s->launches++;
-            }
-        } else {
-            if (s->nrec) {
-                k_receivers<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->traces + (size_t)n * s->nrec, s->f1, s->f2,
-                                                                  s->rec, s->nrec);
-                s->launches++;
-            }
-            FwdStepArgs a{};
-            a.pin = s->f1;
-            a.qin = s->f2;
-            a.pout = s->g1;
-            a.qout = s->g2;
-            a.f3 = s->f3;
-            a.f4 = s->f4;
-            a.m = model_of(s);
-            a.abx = s->abx;
-            a.aby = s->aby;
-            a.abz = s->abz;
-            a.src_index = s->src_index;
-            a.src_term = s->src_index >= 0 ? s->wavelet[n] * c.dt : 0.0f;
-            a.snap = slot;
-            a.snap_prec = c.snap_precision;
-            if (snap && c.snap_precision != SNAP_F32) {
-                float* sc = s->snap_scale + (size_t)(n / c.xcorr_step) * 4;
-                k_snap_scale<<<1, 32, 0, st>>>(sc, s->snap_amax);
-                s->launches++;
-                a.snap_scale = sc;
-                a.snap_amax = s->snap_amax;
-            }
-            a.free_surface = c.free_surface;
-            a.vti = s->vti ? 1 : 0;
-            a.dt = c.dt;
-            a.dx = c.dx;
-            a.dy = c.dy;
-            a.dz = c.dz;
-            mark_begin(s, 0, st);
-            rc = launch_fused_forward(L, a, st);
-            mark_end(s, st);
-            if (rc) return rc;
-            s->launches++;
-            swap_pq(s);
-        }
-        if ((rc = launch_status())) return rc;
-    }
-    if (traces && s->nrec) {
+        return TTI_OK;
+    });
+    if (!rc && traces && s->nrec) {
         size_t bytes = (size_t)s->nrec * c.nt * sizeof(float);
         cudaError_t e = cudaMemcpyAsync(traces, s->traces, bytes,
-                                        traces_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st);
-        if (e != cudaSuccess) return cuda_rc(e);
+                                        traces_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s->stream);
+        if (e != cudaSuccess) rc = cuda_rc(e);
     }
-    rc = cuda_rc(cudaStreamSynchronize(st));
-    if (!rc && fused) rc = fused_wait_status(st);
+    if (rc) {
+        cudaStreamSynchronize(s->stream);
+        return rc;
+    }
+    rc = cuda_rc(cudaStreamSynchronize(s->stream));
+    if (!rc && fused) rc = fused_wait_status(s->stream);
     collect_marks(s);
     if (!rc) s->forward_done = true;
     return rc;
@@ -714,100 +980,73 @@ static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device
     if (!s) return TTI_EINVAL;
     if (!s->model_set || !s->forward_done || !s->cfg.save_snapshots) return TTI_ESTATE;
     const tti_sim_config& c = s->cfg;
-    const Layout& L = s->L;
-    cudaStream_t st = s->stream;
+    cudaStream_t st0 = s->stream;
     s->launches = 0;
-    int rc = TTI_OK;
-    for (float* v : {s->f1, s->f2, s->f3, s->f4, s->g1, s->g2})
-        if (!rc) rc = sim_zero(s, v, s->nvol());
-    if (!rc) rc = sim_zero(s, s->grad_vp, s->ninterior);
-    if (!rc) rc = sim_zero(s, s->grad_rho, s->ninterior);
+    int rc = zero_state(s, s->w);
+    if (!rc) rc = sim_zero(s, s->grad_vp, s->ninterior * sizeof(float));
+    if (!rc) rc = sim_zero(s, s->grad_rho, s->ninterior * sizeof(float));
     if (rc) return rc;
     if (s->nrec && residual) {
         size_t bytes = (size_t)s->nrec * c.nt * sizeof(float);
         cudaError_t e = cudaMemcpyAsync(s->resid, residual, bytes,
-                                        residual_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+                                        residual_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st0);
         if (e != cudaSuccess) return cuda_rc(e);
     } else if (s->nrec) {
-        if ((rc = sim_zero(s, s->resid, (int64_t)s->nrec * c.nt))) return rc;
+        if ((rc = sim_zero(s, s->resid, (size_t)s->nrec * c.nt * sizeof(float)))) return rc;
     }
     const bool fused = c.fused != 0;
-    for (int n = c.nt - 1; n >= 0; --n) {
-        if (s->src_index >= 0) {
-            k_source_trace<<<1, 1, 0, st>>>(s->srctr + n, s->f1, s->f2, s->src_index);
-            s->launches++;
-        }
-        if (s->nrec) {
-            const float* obs = observed ? s->resid + (size_t)n * s->nrec : nullptr;
-            const float* res = observed ? s->traces + (size_t)n * s->nrec : s->resid + (size_t)n * s->nrec;
-            k_inject_residual<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->f3, s->f4, s->rec, res, obs, s->nrec);
-            s->launches++;
-        }
-        if (!fused) {
-            if ((rc = adjoint_per_kernel_step(s, st))) return rc;
-        } else {
-            AdjStepArgs a{};
-            a.pin = s->f1;
-            a.qin = s->f2;
-            a.pout = s->g1;
-            a.qout = s->g2;
-            a.f3 = s->f3;
-            a.f4 = s->f4;
-            a.m = model_of(s);
-            a.abx = s->abx;
-            a.aby = s->aby;
-            a.abz = s->abz;
-            a.sponge_active = s->sponge_active ? 1 : 0;
-            a.free_surface = c.free_surface;
-            a.vti = s->vti ? 1 : 0;
-            a.dt = c.dt;
-            a.dx = c.dx;
-            a.dy = c.dy;
-            a.dz = c.dz;
-            mark_begin(s, 1, st);
-            rc = launch_fused_adjoint(L, a, st);
-            mark_end(s, st);
-            if (rc) return rc;
-            s->launches++;
-            swap_pq(s);
-        }
-        if (n % c.xcorr_step == 0) {
-            const float* slot =
-                static_cast<const float*>(s->snaps) + (size_t)(n / c.xcorr_step) * 4 * s->ninterior;
-            mark_begin(s, 2, st);
-            if (fused && (fused_image_supported(L) || c.snap_precision != SNAP_F32)) {
-                ImageArgs ia{};
-                ia.adj1 = s->f1;
-                ia.adj2 = s->f2;
-                ia.adj3 = s->f3;
-                ia.adj4 = s->f4;
-                ia.store = s->snaps;
-                ia.snap_prec = c.snap_precision;
-                ia.snap_scale = s->snap_scale + (size_t)(n / c.xcorr_step) * 4;
-                ia.nsnap = s->nsnap;
-                ia.slot = n / c.xcorr_step;
-                ia.m = model_of(s);
-                ia.grad_vp = s->grad_vp;
-                ia.grad_rho = s->grad_rho;
-                ia.free_surface = c.free_surface;
-                ia.vti = s->vti ? 1 : 0;
-                ia.dx = c.dx;
-                ia.dy = c.dy;
-                ia.dz = c.dz;
-                rc = launch_fused_image(L, ia, st);
+    auto adjoint_steps = [&](int hi, int lo, int seg_start, cudaStream_t st) -> int {
+        int r = TTI_OK;
+        for (int n = hi; n >= lo; --n) {
+            if (s->src_index >= 0) {
+                k_source_trace<<<1, 1, 0, st>>>(s->srctr + n, s->w.p, s->w.q, s->src_index);
                 s->launches++;
-            } else {
-                rc = image_per_kernel(s, slot, st);
             }
-            mark_end(s, st);
-            if (rc) return rc;
+            if (s->nrec) {
+                const float* obs = observed ? s->resid + (size_t)n * s->nrec : nullptr;
+                const float* res = observed ? s->traces + (size_t)n * s->nrec : s->resid + (size_t)n * s->nrec;
+                k_inject_residual<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->w.pd, s->w.qd, s->rec, res, obs, s->nrec);
+                s->launches++;
+            }
+            if (!fused) {
+                if ((r = adjoint_per_kernel_step(s, st))) return r;
+            } else {
+                if ((r = fused_adjoint_step(s, st))) return r;
+            }
+            if (n % c.xcorr_step == 0 && (r = image_step(s, (n - seg_start) / c.xcorr_step, st))) return r;
+            if ((r = launch_status())) return r;
         }
-        if ((rc = launch_status())) return rc;
+        return TTI_OK;
+    };
+    if (!s->ckpt) {
+        rc = run_on_stream(s, 1, [&](cudaStream_t st) { return adjoint_steps(c.nt - 1, 0, 0, st); });
+    } else {
+        // segments from the last to the first; the last one's snapshots are
+        // still in the store from the forward pass
+        const int nseg = (c.nt - 1) / s->ckpt + 1;
+        for (int k = nseg - 1; k >= 0 && !rc; --k) {
+            const int a = k * s->ckpt, b = std::min(c.nt, a + s->ckpt);
+            rc = run_on_stream(s, k == nseg - 1 ? 1 : 2, [&](cudaStream_t st) -> int {
+                int r = TTI_OK;
+                if (k != nseg - 1) {
+                    if ((r = restore_checkpoint(s, s->rw, k, st))) return r;
+                    for (int n = a; n < b; ++n) {
+                        const int slot = (n % c.xcorr_step == 0) ? (n - a) / c.xcorr_step : -1;
+                        if ((r = fused_forward_step(s, s->rw, n, slot, st))) return r;
+                    }
+                }
+                return adjoint_steps(b - 1, a, a, st);
+            });
+        }
     }
-    k_finalize_dense<<<s->dense_grid(), 128, 0, st>>>(s->grad_vp, s->mv[3], L, c.dt * c.xcorr_step);
+    if (rc) {
+        cudaStreamSynchronize(st0);
+        return rc;
+    }
+    k_finalize_dense<<<s->dense_grid(), 128, 0, st0>>>(s->grad_vp, s->mv[3], s->L, c.dt * c.xcorr_step);
     s->launches++;
-    rc = cuda_rc(cudaStreamSynchronize(st));
-    if (!rc && fused) rc = fused_wait_status(st);
+    rc = cuda_rc(cudaStreamSynchronize(st0));
+    if (!rc && fused) rc = fused_wait_status(st0);
     collect_marks(s);
     return rc;
 }
@@ -862,7 +1101,7 @@ int tti_sim_source_gradient(tti_sim* s, float* host_out)
 int tti_sim_volume(tti_sim* s, int which, float** dev_ptr)
 {
     if (!s || !dev_ptr || which < 0 || which > 11) return TTI_EINVAL;
-    float* v[12] = {s->f1, s->f2, s->f3, s->f4, s->mv[0], s->mv[1], s->mv[2], s->mv[3],
+    float* v[12] = {s->w.p, s->w.q, s->w.pd, s->w.qd, s->mv[0], s->mv[1], s->mv[2], s->mv[3],
                     s->mv[4], s->mv[5], s->mv[6], s->mv[7]};
     *dev_ptr = v[which];
     return TTI_OK;

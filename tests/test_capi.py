@@ -78,3 +78,34 @@ def test_reduced_precision_snapshots_need_the_fused_path():
     with pytest.raises(P.TTIError) as e:  # nx not a multiple of 8
         P.Simulator(P.Config(nx=44, ny=40, nz=40, nt=8, snap_precision="bf16"))
     assert e.value.status == P.EINVAL
+
+
+def test_checkpoint_config_is_validated():
+    base = dict(nx=32, ny=24, nz=24, nt=40, xcorr_step=4)
+    for bad in (dict(checkpoint_every=6), dict(checkpoint_every=8, fused=False),
+                dict(checkpoint_every=8, save_snapshots=False), dict(checkpoint_every=-4)):
+        with pytest.raises(P.TTIError) as e:
+            P.Config(**base, **bad).footprint_bytes()
+        assert e.value.status == P.EINVAL
+
+
+def test_footprint_accounts_for_snapshots_and_checkpoints():
+    """The footprint query needs no device: it is the creation plan's sum."""
+    n = 64 * 64 * 64
+    lay = (96, 72, 72)
+    vol = lay[0] * lay[1] * lay[2] * 4
+    cfg = dict(nx=64, ny=64, nz=64, nt=400, xcorr_step=4)
+    full = P.Config(**cfg).footprint_bytes()
+    nsnap = 100
+    assert full >= 14 * vol + nsnap * 4 * n * 4
+    half = P.Config(**cfg, snap_precision="fp16").footprint_bytes()
+    assert full - half == nsnap * 4 * n * 2 + 0  # same plan but 2-byte slots
+    ck = P.Config(**cfg, snap_precision="fp16", checkpoint_every=40).footprint_bytes()
+    # 10 FP32 checkpoints + one 10-slot segment + the recompute state
+    assert ck < half
+    assert ck - (half - nsnap * 4 * n * 2) == pytest.approx(
+        10 * 4 * n * 4 + 10 * 4 + 10 * 4 * n * 2 + 6 * vol, abs=4096)
+    no_snap = P.Config(**cfg, save_snapshots=False).footprint_bytes()
+    assert no_snap < ck
+    # the reference kernel sequence needs its derivative volumes and scratch
+    assert P.Config(**cfg, save_snapshots=False, fused=False).footprint_bytes() - no_snap == 14 * vol
