@@ -40,7 +40,8 @@ enum {
     TTI_ELAUNCH = 3,  /* kernel launch or CUDA runtime error */
     TTI_ETIMEOUT = 4, /* a bounded wait gave up */
     TTI_ESTATE = 5,   /* call out of order (e.g. read before any write) */
-    TTI_ERANGE = 6    /* a reduced-precision snapshot value saturated (results produced) */
+    TTI_ERANGE = 6,   /* a reduced-precision snapshot value saturated (results produced) */
+    TTI_ETOOBIG = 7   /* request larger than a fixed-capacity buffer of the library */
 };
 
 typedef void* tti_stream_t;
@@ -93,6 +94,27 @@ int tti_launch_adj_kernel2_drv(float* dfield1dx, float* dfield2dx, float* dfield
                                int iyend, int izbeg, int izend, float invdxx, float invdyy, float invdzz,
                                float invdxy, float invdyz, float invdzx, int ldimx, int ldimy, int order, float dt,
                                float invdx, float invdy, float invdz, tti_stream_t stream);
+
+/* Same computation and arguments as tti_launch_adj_kernel2_drv, with a
+ * scratch that is never allocated: no counterpart in the reference.  For
+ * callers that must not have the library allocate device memory (their own
+ * pool holds HBM, or they cannot take the device-wide synchronize of a
+ * growing scratch).  The scratch is a fixed array of
+ * TTI_NOALLOC_SCRATCH_CELLS cells (16 MiB); a request with
+ * ldimx * ldimy * (izend + 5) above that returns TTI_ETOOBIG.  The first
+ * call on a device looks up the array's address and should come before any
+ * stream capture.  All calls on a device share the array: calls that overlap
+ * on the GPU race and must be ordered by the caller. */
+#define TTI_NOALLOC_SCRATCH_CELLS (1 << 20)
+int tti_launch_adj_kernel2_drv_noalloc(float* dfield1dx, float* dfield2dx, float* dfield1dy, float* dfield2dy,
+                                       float* dfield1dz, float* dfield2dz, float* field3_rhs, float* field4_rhs,
+                                       const float* field1, const float* field2, const float* Model11,
+                                       const float* model1, const float* model2, const float* model3,
+                                       const float* model4, const float* model5, const float* model6,
+                                       const float* model7, int ixbeg, int ixend, int iybeg, int iyend, int izbeg,
+                                       int izend, float invdxx, float invdyy, float invdzz, float invdxy,
+                                       float invdyz, float invdzx, int ldimx, int ldimy, int order, float dt,
+                                       float invdx, float invdy, float invdz, tti_stream_t stream);
 
 /* Adjoint update.  Replaces kernel3_gpu_kernels::launch_update_adj_kernel_main_3
  * (kernels/kernel_type2_adj.h:8-14).  ab_* are float2 (A,B) sponge arrays

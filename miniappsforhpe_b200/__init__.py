@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtti_b200.so")
 RADIUS = 4
 
-OK, EINVAL, ENOMEM, ELAUNCH, ETIMEOUT, ESTATE, ERANGE = range(7)
+OK, EINVAL, ENOMEM, ELAUNCH, ETIMEOUT, ESTATE, ERANGE, ETOOBIG = range(8)
 
 
 class TTIError(RuntimeError):

@@ -584,6 +584,7 @@ const char* tti_status_string(int status)
     case TTI_ETIMEOUT: return "timed out";
     case TTI_ESTATE: return "call out of order";
     case TTI_ERANGE: return "reduced-precision snapshot saturated";
+    case TTI_ETOOBIG: return "request exceeds a fixed-capacity buffer";
     default: return "unknown status";
     }
 }

@@ -1,0 +1,69 @@
+"""tti_launch_adj_kernel2_drv_noalloc: the adjoint-derivative launcher whose
+scratch is a fixed device array instead of library-allocated memory.
+
+Called through the C ABI on two inputs in a row (the second call finds the
+first one's scratch contents) and compared with tti_launch_adj_kernel2_drv on
+the same inputs, at the 1e-5 relative L2 tolerance of the parity tests.  A
+range larger than the array is rejected before anything runs."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import miniappsforhpe_b200 as P
+from oracle import Layout
+from tests.helpers import random_field, random_model, rel_l2
+
+NOALLOC_CELLS = 1 << 20  # TTI_NOALLOC_SCRATCH_CELLS
+SIG = [C.c_void_p] * 18 + [C.c_int] * 6 + [C.c_float] * 6 + [C.c_int] * 3 + [C.c_float] * 4 + [C.c_void_p]
+
+
+def entry(name):
+    f = getattr(P.lib(), name)
+    f.argtypes = SIG
+    f.restype = C.c_int
+    return f
+
+
+def run(fn, torch, lay, rng_seed, dx=10.0, dy=12.0, dz=8.0):
+    rng = np.random.default_rng(rng_seed)
+    m = random_model(lay, rng, tti=True)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    f1, f2 = dev(random_field(lay, rng)), dev(random_field(lay, rng))
+    mv = {k: dev(v) for k, v in m.items()}
+    outs = [torch.zeros(lay.shape, dtype=torch.float32, device="cuda") for _ in range(8)]
+    xb, xe, yb, ye, zb, ze = lay.ranges
+    rc = fn(*[o.data_ptr() for o in outs], f1.data_ptr(), f2.data_ptr(), mv["irho"].data_ptr(),
+            mv["m1"].data_ptr(), mv["m2"].data_ptr(), mv["m3"].data_ptr(), mv["m4"].data_ptr(),
+            mv["rx"].data_ptr(), mv["ry"].data_ptr(), mv["rz"].data_ptr(), xb, xe, yb, ye, zb, ze,
+            1 / dx**2, 1 / dy**2, 1 / dz**2, 1 / (4 * dx * dy), 1 / (4 * dy * dz), 1 / (4 * dx * dz),
+            lay.ldimx, lay.ldimy, 8, 1e-3, 1 / dx, 1 / dy, 1 / dz, None)
+    torch.cuda.synchronize()
+    return rc, [o.cpu().numpy() for o in outs]
+
+
+@pytest.mark.gpu
+def test_noalloc_adjoint_derivatives_match_the_allocating_entry_point():
+    import torch
+    noalloc = entry("tti_launch_adj_kernel2_drv_noalloc")
+    alloc = entry("tti_launch_adj_kernel2_drv")
+    # two calls in a row: a larger grid, then a smaller one with other values
+    for (nx, ny, nz), seed in (((40, 36, 30), 11), ((28, 22, 20), 12)):
+        lay = Layout(nx, ny, nz)
+        assert lay.ldimx * lay.ldimy * (lay.ranges[5] + 5) <= NOALLOC_CELLS
+        rc_a, want = run(alloc, torch, lay, seed)
+        rc_n, got = run(noalloc, torch, lay, seed)
+        assert rc_a == P.OK and rc_n == P.OK
+        for g, w in zip(got, want):
+            assert np.abs(w).max() > 0
+            assert rel_l2(g, w) < 1e-5
+
+    # a range beyond the fixed scratch is refused with its own status
+    lay = Layout(120, 120, 80)
+    assert lay.ldimx * lay.ldimy * (lay.ranges[5] + 5) > NOALLOC_CELLS
+    small = torch.zeros(16, dtype=torch.float32, device="cuda")
+    xb, xe, yb, ye, zb, ze = lay.ranges
+    rc = noalloc(*([small.data_ptr()] * 18), xb, xe, yb, ye, zb, ze, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0,
+                 lay.ldimx, lay.ldimy, 8, 1e-3, 1.0, 1.0, 1.0, None)
+    assert rc == P.ETOOBIG
+    assert P.status_string(rc) == "request exceeds a fixed-capacity buffer"
