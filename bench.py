@@ -50,6 +50,23 @@ def parse():
     ap.add_argument("--per-kernel", action="store_true", help="reference kernel sequence instead of fused")
     ap.add_argument("--snap-precision", choices=["fp32", "fp16", "bf16"], default="fp32",
                     help="snapshot storage (the stencils and time update stay FP32)")
+    ap.add_argument("--checkpoint", type=int, default=0,
+                    help="checkpointed recomputation: FP32 checkpoints every K steps")
+    ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="non-cubic grid (overrides --n)")
+    ap.add_argument("--f0", type=float, default=12.0, help="Ricker peak frequency (Hz)")
+    ap.add_argument("--dx", type=float, default=10.0)
+    ap.add_argument("--model", choices=["smooth", "layered"], default="smooth",
+                    help="smooth Gaussian-random TTI (full RTM workload) or layered VTI")
+    ap.add_argument("--serve", action="store_true",
+                    help="served batch: Poisson stream of RTM shots through the shot server, "
+                         "against the same stream run one shot at a time in plain FP32")
+    ap.add_argument("--shots", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=2.0, help="mean arrivals per second")
+    ap.add_argument("--nt-range", type=int, nargs=2, default=[1000, 3000])
+    ap.add_argument("--max-active", type=int, default=8)
+    ap.add_argument("--round-ms", type=float, default=50.0)
+    ap.add_argument("--serve-modes", default="served,sequential")
     return ap.parse_args()
 
 
@@ -60,23 +77,36 @@ def dist_env():
     return ws, rank, local
 
 
+def grid_of(args):
+    return tuple(args.grid) if args.grid else (args.n, args.n, args.n)
+
+
 def workload(args, rank):
     from miniappsforhpe_b200 import earth_models as EM
 
-    n = args.n
-    model = EM.smooth_tti(n, n, n, dx=10.0, corr_m=300.0, seed=1234 + rank)
-    true = EM.add_velocity_blob(model, (n // 2, n // 2, n // 2), radius_cells=max(2, n // 12), fraction=0.05)
-    dt = EM.cfl_dt(true, 10.0, cfl=0.4)
-    w = EM.ricker(args.nt, dt, 12.0)
-    src = (n // 2 + (rank * 17) % max(1, n // 4), n // 2, 5)
-    rec = EM.receiver_plane(n, n, 3)
+    nx, ny, nz = grid_of(args)
+    if args.model == "layered":
+        model = EM.layered_vti(nx, ny, nz, nlayers=6, seed=1234 + rank)
+        mdesc = "layered VTI (6 flat layers), observed = model + 5% vp blob"
+    else:
+        model = EM.smooth_tti(nx, ny, nz, dx=args.dx, corr_m=300.0, seed=1234 + rank)
+        mdesc = "smooth Gaussian-random TTI (300 m), observed = model + 5% vp blob"
+    true = EM.add_velocity_blob(model, (nx // 2, ny // 2, nz // 2), radius_cells=max(2, min(nx, ny, nz) // 12),
+                                fraction=0.05)
+    dt = EM.cfl_dt(true, args.dx, cfl=0.4)
+    w = EM.ricker(args.nt, dt, args.f0)
+    src = (nx // 2 + (rank * 17) % max(1, nx // 4), ny // 2, 5)
+    rec = EM.receiver_plane(nx, ny, 3)
+    gname = f"{nx}^3" if nx == ny == nz else f"{nx}x{ny}x{nz}"
     desc = {
-        "workload": f"TTI RTM shot {n}^3, dx=10m, sponge 24, {args.nt} steps, imaging every {args.xcorr}",
-        "grid": [n, n, n], "nt": args.nt, "xcorr_step": args.xcorr, "sponge_width": 24,
-        "model": "smooth Gaussian-random TTI (300 m), observed = model + 5% vp blob",
-        "source": "12 Hz Ricker", "receivers": f"{n * n} (plane z=3)",
+        "workload": (f"TTI RTM shot {gname}, dx={args.dx:g}m, sponge 24, {args.nt} steps, imaging every "
+                     f"{args.xcorr}"),
+        "grid": [nx, ny, nz], "nt": args.nt, "xcorr_step": args.xcorr, "sponge_width": 24, "dx": args.dx,
+        "model": mdesc, "source": f"{args.f0:g} Hz Ricker", "receivers": f"{nx * ny} (plane z=3)",
         "l2": "inputs larger than L2 (every step streams >1 GB through HBM)",
     }
+    if args.checkpoint:
+        desc["checkpoint_every"] = args.checkpoint
     return model, true, dt, w, src, rec, desc
 
 
@@ -221,10 +251,11 @@ def run_ours(args):
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
     model, true, dt, w, src, rec, desc = workload(args, rank)
-    n = args.n
-    cfg = P.Config(nx=n, ny=n, nz=n, dx=10.0, dy=10.0, dz=10.0, dt=dt, nt=args.nt, xcorr_step=args.xcorr,
-                   sponge_width=24, free_surface=True, fused=not args.per_kernel, save_snapshots=True,
-                   snap_precision=args.snap_precision)
+    nx, ny, nz = grid_of(args)
+    npts = float(nx) * ny * nz
+    cfg = P.Config(nx=nx, ny=ny, nz=nz, dx=args.dx, dy=args.dx, dz=args.dx, dt=dt, nt=args.nt,
+                   xcorr_step=args.xcorr, sponge_width=24, free_surface=True, fused=not args.per_kernel,
+                   save_snapshots=True, snap_precision=args.snap_precision, checkpoint_every=args.checkpoint)
     sim = P.Simulator(cfg)
     sim.set_source(*src, w)
     sim.set_receivers(rec)
@@ -234,7 +265,7 @@ def run_ours(args):
     observed = torch.empty((args.nt, nrec), dtype=torch.float32, device=dev)
     sim.forward(observed)
     sim.set_model(**model)
-    gvp = torch.empty((n, n, n), dtype=torch.float32, device=dev)
+    gvp = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev)
     grho = torch.empty_like(gvp)
     synth = torch.empty_like(observed)
     stack = torch.zeros_like(gvp)
@@ -280,7 +311,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
-    pts = float(n) ** 3 * args.nt
+    pts = npts * args.nt
     value = pts * args.steps * ws / (ms / 1e3) / 1e9
     ms_per_step = ms / args.steps
 
@@ -289,16 +320,16 @@ def run_ours(args):
     kind = max(("forward", "adjoint"), key=lambda k: times[k][0])
     kms, kn = times[kind]
     per_launch_s = (kms / max(kn, 1)) / 1e3
-    alg_bytes = (B_FWD if kind == "forward" else B_ADJ) * float(n) ** 3
+    alg_bytes = (B_FWD if kind == "forward" else B_ADJ) * npts
     achieved = alg_bytes / per_launch_s / 1e9 if kn else None
-    traffic = ncu_traffic().get(f"{kind}_dram_bytes_per_launch_{n}")
+    traffic = ncu_traffic().get(f"{kind}_dram_bytes_per_launch_{nx}x{ny}x{nz}")
     roofline = {"kernel": f"fused {kind} step", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                 "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
                 "avg_launch_ms": per_launch_s * 1e3, "launches": kn}
     passes = {k: {"total_ms": v[0] / args.steps, "launches_per_shot": v[1] / args.steps}
               for k, v in times.items()}
-    step_bytes = (B_FWD + B_ADJ + B_IMG / args.xcorr + B_SNAP / args.xcorr) * float(n) ** 3
+    step_bytes = (B_FWD + B_ADJ + B_IMG / args.xcorr + B_SNAP / args.xcorr) * npts
     hbm_frac = step_bytes * args.nt / (ms_per_step / 1e3) / 1e9 / peak
 
     # end to end through the host-buffer API
@@ -321,8 +352,8 @@ def run_ours(args):
             t = torch.tensor([el], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             el = float(t.item())
-        h2d = 7 * n ** 3 * 4 + args.nt * nrec * 4
-        d2h = args.nt * nrec * 4 + 2 * n ** 3 * 4
+        h2d = int(7 * npts * 4 + args.nt * nrec * 4)
+        d2h = int(args.nt * nrec * 4 + 2 * npts * 4)
         e2e = {"value": pts * args.steps * ws / el / 1e9, "unit": "Gpts/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "timer": "wall clock, synchronized on both sides"}
         del tr, gv, gr
@@ -353,8 +384,149 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+SERVE_SIZES = [(96, 96, 96), (160, 160, 160), (224, 224, 160), (320, 320, 200)]
+
+
+def serve_stream(args):
+    """The served batch: arrival time, grid, steps, source and model seed per shot."""
+    rng = np.random.default_rng(2024)
+    t = np.cumsum(rng.exponential(1.0 / args.rate, args.shots))
+    t -= t[0]
+    out = []
+    for i in range(args.shots):
+        nx, ny, nz = SERVE_SIZES[rng.integers(len(SERVE_SIZES))]
+        nt = int(rng.integers(args.nt_range[0], args.nt_range[1] + 1))
+        src = (int(rng.integers(0, nx)), int(rng.integers(0, ny)), 2)
+        out.append(dict(i=i, arrival=float(t[i]), nx=nx, ny=ny, nz=nz, nt=nt, src=src, seed=1000 + i))
+    return out
+
+
+def serve_shot(spec, keep_traces=False):
+    """Shot object for one stream entry: layered VTI model of the seed (6 flat
+    layers, vp 1500-4500, eps U[0,0.3], delta U[0,min(0.15,eps)]), 20-cell
+    sponge, 15 Hz Ricker, dt from CFL 0.4, receivers every 4th cell of z=3."""
+    from miniappsforhpe_b200 import earth_models as EM
+    from miniappsforhpe_b200.serve import Shot
+
+    nx, ny, nz, nt = spec["nx"], spec["ny"], spec["nz"], spec["nt"]
+    m = EM.layered_vti(nx, ny, nz, nlayers=6, seed=spec["seed"])
+    dt = EM.cfl_dt(m, 10.0, cfl=0.4)
+    w = EM.ricker(nt, dt, 15.0) * 1e3
+    rec = EM.receiver_plane(nx, ny, 3)
+    rec = rec[(rec[:, 0] % 4 == 0) & (rec[:, 1] % 4 == 0)]
+    return Shot(nx=nx, ny=ny, nz=nz, dt=dt, nt=nt, vp=m["vp"], eps=m["eps"], delta=m["delta"], wavelet=w,
+                source=spec["src"], receivers=rec, sponge_width=20, want_traces=keep_traces)
+
+
+def serve_run(args, stream, mode, keep):
+    """Play the stream against a server; returns per-shot records."""
+    import threading
+
+    from miniappsforhpe_b200.serve import Server
+
+    if mode == "served":
+        srv = Server(max_active=args.max_active, round_ms=args.round_ms, use_graphs=True, autotune=True,
+                     snap_precision="fp16")
+    else:
+        srv = Server(max_active=1, round_ms=200.0, use_graphs=False, autotune=False, snap_precision="fp32")
+    # warm-up: one short shot per grid size (first-sight tuning and cost model)
+    warm = []
+    for k, (nx, ny, nz) in enumerate(SERVE_SIZES):
+        spec = dict(i=-1, arrival=0.0, nx=nx, ny=ny, nz=nz, nt=16, src=(nx // 2, ny // 2, 2), seed=77 + k)
+        sh = serve_shot(spec)
+        warm.append((srv.submit(sh), sh))
+    for t, _ in warm:
+        srv.wait(t)
+    tickets = {}
+    errors = []
+
+    def client():
+        t0 = time.perf_counter()
+        for spec in stream:
+            sh = serve_shot(spec)
+            dly = spec["arrival"] - (time.perf_counter() - t0)
+            if dly > 0:
+                time.sleep(dly)
+            try:
+                tickets[spec["i"]] = (srv.submit(sh), sh)
+            except Exception as e:  # noqa: BLE001
+                errors.append(repr(e))
+                return
+
+    th = threading.Thread(target=client)
+    th.start()
+    recs = []
+    for spec in stream:
+        while spec["i"] not in tickets:
+            if errors:
+                raise RuntimeError(errors[0])
+            time.sleep(0.002)
+        t, sh = tickets[spec["i"]]
+        r = srv.wait(t)
+        if r.status != 0:
+            raise RuntimeError(f"shot {spec['i']} failed with status {r.status}")
+        rec = dict(i=spec["i"], t_submit=r.t_submit, t_admit=r.t_admit, t_done=r.t_done, latency=r.latency,
+                   ckpt=r.checkpoint_every, units=r.units, footprint=r.footprint)
+        if spec["i"] in keep:
+            rec["image"] = (sh.image_vp.copy(), sh.image_rho.copy())
+        recs.append(rec)
+        tickets[spec["i"]] = None
+    th.join()
+    stats = srv.stats()
+    srv.close()
+    return recs, stats
+
+
+def serve_summary(recs, stats, stream):
+    lat = np.array([r["latency"] for r in recs])
+    span = max(r["t_done"] for r in recs) - min(r["t_submit"] for r in recs)
+    pts = sum(s["nx"] * s["ny"] * s["nz"] * s["nt"] for s in stream)
+    return {"shots": len(recs), "shots_per_hour": len(recs) / span * 3600.0, "makespan_s": span,
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "mean_latency_s": float(lat.mean()), "gpts_per_s": pts / span / 1e9,
+            "checkpointed_shots": int(sum(1 for r in recs if r["ckpt"])),
+            "device_busy_frac": stats["busy_ms"] / 1e3 / span, "rounds": stats["rounds"],
+            "graph_updates": stats["graph_updates"], "graph_instantiations": stats["graph_instantiations"],
+            "max_resident": stats["max_resident"]}
+
+
+def run_serve(args):
+    stream = serve_stream(args)
+    keep = {s["i"] for s in stream if s["i"] % 4 == 0}
+    modes = [m for m in args.serve_modes.split(",") if m]
+    out, images = {}, {}
+    for mode in modes:
+        recs, stats = serve_run(args, stream, mode, keep)
+        out[mode] = serve_summary(recs, stats, stream)
+        images[mode] = {r["i"]: r["image"] for r in recs if "image" in r}
+    line = {"metric": METRIC, "mode": "serve", "unit": "shots/hour",
+            "value": out.get("served", out.get(modes[0]))["shots_per_hour"], "higher_is_better": True,
+            "n_gpus": 1, "dtype": "f32 stencils, fp16 snapshots (served) / fp32 (sequential)",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"served batch: {args.shots} TTI RTM shots, Poisson arrivals {args.rate}/s",
+                       "sizes": SERVE_SIZES, "nt_range": args.nt_range, "max_active": args.max_active,
+                       "round_ms": args.round_ms, "model": "layered VTI per shot seed (6 layers), 15 Hz Ricker",
+                       "receivers": "every 4th cell of plane z=3", "sponge_width": 20,
+                       "observed": "zero (residual = synthetic traces; work does not depend on the values)"},
+            **out}
+    if "served" in out and "sequential" in out:
+        line["speedup_shots_per_hour"] = out["served"]["shots_per_hour"] / out["sequential"]["shots_per_hour"]
+        e = []
+        for i, (gv, gr) in images["served"].items():
+            rv, rr = images["sequential"][i]
+            e.append((float(np.linalg.norm((gv - rv).astype(np.float64)) / max(np.linalg.norm(rv), 1e-30)),
+                      float(np.linalg.norm((gr - rr).astype(np.float64)) / max(np.linalg.norm(rr), 1e-30))))
+        line["image_rel_l2_served_vs_fp32"] = {"shots_compared": len(e), "max_vp": max(x[0] for x in e),
+                                               "max_rho": max(x[1] for x in e)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.serve:
+        run_serve(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

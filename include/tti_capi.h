@@ -249,6 +249,29 @@ int tti_sim_adjoint(tti_sim* sim, const float* residual, int residual_on_device)
  * traces of the last forward run minus these observed traces (nt*nrec). */
 int tti_sim_adjoint_observed(tti_sim* sim, const float* observed, int observed_on_device);
 
+/* z-chunk autotuner.  The fused kernels run one CTA per SM on a
+ * TX x TY x bz block of outputs (TX = 32, TY = 16) marching along z; bz sets
+ * how many CTAs a step launches against the pipeline fill of each chunk.
+ * tti_sim_autotune times every candidate bz (ceil(nz/n) >= 8) of the fused
+ * forward, adjoint and (with a snapshot store) imaging kernels on this
+ * simulator's volumes, reps launches each, and records the fastest for this
+ * grid on the current device; later launches on any simulator of the same
+ * grid use it.  Needs fused = 1 and a model.  Wavefield and image contents
+ * afterwards are unspecified (forward and adjoint start from zero). */
+typedef struct {
+    int bz[3];         /* chosen bz: forward, adjoint, imaging (0: not tuned) */
+    float ms[3];       /* per-launch time at the chosen bz */
+    float model_ms[3]; /* per-launch time at the wave-count model's bz */
+    int ncand;         /* candidates tried per kernel */
+} tti_tune_report;
+int tti_sim_autotune(tti_sim* sim, int reps, tti_tune_report* out);
+
+/* Record (bz > 0) or clear (bz = 0) the z-chunk used for kernel kind
+ * (0 forward, 1 adjoint, 2 imaging) on an nx*ny*nz grid, current device;
+ * tti_tune_get returns the bz in effect (recorded or modelled). */
+int tti_tune_set(int nx, int ny, int nz, int kind, int bz);
+int tti_tune_get(int nx, int ny, int nz, int kind);
+
 /* Image readback: Vp gradient (finalised, -2*dt*xcorr/vp) and rho gradient,
  * nx*ny*nz each, host or device memory. */
 int tti_sim_get_image(tti_sim* sim, float* grad_vp, float* grad_rho, int on_device);
@@ -303,6 +326,80 @@ int tti_snap_start_read(tti_snap_store* s, float* const* vols, tti_stream_t stre
 /* Orders stream after the pending read (rtm_snap finish_read). */
 int tti_snap_finish_read(tti_snap_store* s, tti_stream_t stream);
 int tti_snap_count(tti_snap_store* s);
+
+/* ------------------------------------------------------------------------
+ * 4. Shot server: continuous batching of RTM shots on one device.  No
+ *    counterpart in the reference (one shot per run there).
+ *
+ *    Shots of any grid size are queued, admitted first-fit in arrival order
+ *    while the number of resident shots is below max_active and their device
+ *    footprint (tti_sim_footprint_bytes plus receiver and set-up buffers)
+ *    fits the HBM budget, and then stay resident (wavefields, snapshot store,
+ *    checkpoints) until their image is read back.  A shot that would not fit
+ *    the budget alone gets checkpointed recomputation.  The scheduler runs in
+ *    rounds: each round advances every resident shot by a number of fused
+ *    steps sized to take about round_ms of device time, all shots in
+ *    parallel branches of one launch (one captured CUDA graph when
+ *    use_graphs = 1); the next round is prepared while the current one runs,
+ *    and shots admitted in the meantime join it.  Each shot computes exactly
+ *    what tti_sim_forward + tti_sim_adjoint_observed compute for it alone.
+ * ---------------------------------------------------------------------- */
+typedef struct tti_server tti_server;
+
+typedef struct {
+    int max_active;      /* shots resident at once (>= 1) */
+    int64_t hbm_budget;  /* device bytes for shots; 0 = free memory at creation minus 2 GiB */
+    float round_ms;      /* target device time of one round (> 0) */
+    int use_graphs;      /* 1: one captured graph launch per round */
+    int autotune;        /* 1: tune the z-chunk of each new grid size before its first shot */
+    int snap_precision;  /* snapshot store of every shot: 0 FP32, 1 FP16, 2 BF16 */
+} tti_server_config;
+
+/* One shot.  Host arrays only; the server reads and writes them while the
+ * shot is queued or resident, so they must stay valid until its result has
+ * been taken with tti_server_wait. */
+typedef struct {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    float dt;
+    int nt, xcorr_step, sponge_width, free_surface;
+    const float *vp, *eps, *delta, *vs, *theta, *phi, *rho; /* nx*ny*nz; NULL = default */
+    int src_ix, src_iy, src_iz;
+    const float* wavelet;  /* nt */
+    int nrec;
+    const int* rec_ixyz;   /* 3*nrec */
+    const float* observed; /* nt*nrec observed traces; NULL = zero (residual = synthetic) */
+    float* image_vp;       /* out, nx*ny*nz, may be NULL */
+    float* image_rho;      /* out, nx*ny*nz, may be NULL */
+    float* traces;         /* out, nt*nrec synthetic traces, may be NULL */
+} tti_shot_request;
+
+typedef struct {
+    int status;                       /* TTI_OK or the failing call's status */
+    double t_submit, t_admit, t_done; /* seconds on the server's clock (tti_server_now) */
+    int64_t footprint;                /* device bytes reserved for the shot */
+    int checkpoint_every;             /* 0 or the segment length chosen at admission */
+    int64_t units;                    /* fused steps run (forward, recomputed, adjoint) */
+    int64_t launches;                 /* kernel launches of the shot */
+} tti_shot_result;
+
+typedef struct {
+    int64_t rounds;               /* batched launches */
+    int64_t graph_updates;        /* rounds whose graph was updated in place */
+    int64_t graph_instantiations;
+    int max_resident;             /* most shots resident at once */
+    double busy_ms;               /* device time of all rounds */
+} tti_server_stats;
+
+int tti_server_create(const tti_server_config* cfg, tti_server** out);
+int tti_server_submit(tti_server* srv, const tti_shot_request* req, int64_t* ticket);
+/* Waits up to timeout_s seconds (< 0: no limit) for the shot; TTI_ETIMEOUT
+ * if it is not done by then.  A result is handed out once. */
+int tti_server_wait(tti_server* srv, int64_t ticket, double timeout_s, tti_shot_result* out);
+int tti_server_stats_get(tti_server* srv, tti_server_stats* out);
+double tti_server_now(tti_server* srv);
+/* Runs every submitted shot to completion, then releases the server. */
+int tti_server_destroy(tti_server* srv);
 
 #ifdef __cplusplus
 }

@@ -61,6 +61,10 @@ class SimConfig(C.Structure):
     ]
 
 
+class TuneReport(C.Structure):
+    _fields_ = [("bz", I * 3), ("ms", F * 3), ("model_ms", F * 3), ("ncand", I)]
+
+
 _SIGS = {
     "tti_launch_fwd_kernel2_drv": [V] * 9 + [I] * 6 + [F] * 3 + [I, I, I, V],
     "tti_launch_update_rho_fwd_main_loop_2_1": [V] * 30 + [I] * 8 + [F, D, D, D, I, I, I, I, I, V],
@@ -87,6 +91,9 @@ _SIGS = {
     "tti_sim_adjoint_observed": [V, V, I],
     "tti_sim_set_profiling": [V, I],
     "tti_sim_kernel_times": [V, V, V],
+    "tti_sim_autotune": [V, I, C.POINTER(TuneReport)],
+    "tti_tune_set": [I, I, I, I, I],
+    "tti_tune_get": [I, I, I, I],
     "tti_sim_volume": [V, I, C.POINTER(V)],
     "tti_sim_read_volume": [V, I, V],
     "tti_sim_layout": [V, C.POINTER(I), C.POINTER(I), C.POINTER(I)],
@@ -394,6 +401,15 @@ class Simulator:
         self._chk(lib().tti_sim_kernel_times(self._h, C.cast(ms, V), C.cast(n, V)), "tti_sim_kernel_times")
         return {k: (ms[i], n[i]) for i, k in enumerate(("forward", "adjoint", "imaging"))}
 
+    def autotune(self, reps: int = 3) -> dict:
+        """Time every z-chunk candidate of the fused kernels on this grid and
+        record the fastest (include/tti_capi.h, tti_sim_autotune)."""
+        r = TuneReport()
+        self._chk(lib().tti_sim_autotune(self._h, int(reps), C.byref(r)), "tti_sim_autotune")
+        kinds = ("forward", "adjoint", "imaging")
+        return {k: {"bz": r.bz[i], "ms": r.ms[i], "model_ms": r.model_ms[i]} for i, k in enumerate(kinds)
+                if r.bz[i] > 0} | {"candidates": r.ncand}
+
     def image(self, out_vp=None, out_rho=None):
         """(grad_vp, grad_rho), each (nz, ny, nx); CUDA tensors if given."""
         if out_vp is not None:
@@ -426,6 +442,23 @@ class Simulator:
 
     def stream_handle(self) -> int:
         return int(lib().tti_sim_stream(self._h) or 0)
+
+
+def tune_set(nx: int, ny: int, nz: int, kind: str, bz: int) -> None:
+    """Record (bz > 0) or clear (bz = 0) the z-chunk of a fused kernel kind
+    ('forward' | 'adjoint' | 'imaging') on an nx*ny*nz grid (current device)."""
+    k = ("forward", "adjoint", "imaging").index(kind)
+    rc = lib().tti_tune_set(nx, ny, nz, k, bz)
+    if rc != OK:
+        raise TTIError(rc, "tti_tune_set")
+
+
+def tune_get(nx: int, ny: int, nz: int, kind: str) -> int:
+    k = ("forward", "adjoint", "imaging").index(kind)
+    v = lib().tti_tune_get(nx, ny, nz, k)
+    if v < 0:
+        raise TTIError(-v, "tti_tune_get")
+    return v
 
 
 class SnapshotStore:

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
@@ -332,7 +333,8 @@ __global__ void __launch_bounds__(NT, 1)
                 }
             };
             dx_at(ty, tx);
-            if (tx < IW - TX) dx_at(ty, tx + TX);
+            // the (IW-TX) x TY halo columns, by whole warps
+            if (tid < (IW - TX) * TY) dx_at(tid / (IW - TX), TX + tid % (IW - TX));
             dy_at(ty, tx);
             if (ty < IH - TY) dy_at(ty + TY, tx);
             __syncthreads();
@@ -691,10 +693,9 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
         };
         temps_at(ty, tx);
         temps_at(ty + TY, tx);
-        if (tx < PW - TX) {
-            temps_at(ty, tx + TX);
-            temps_at(ty + TY, tx + TX);
-        }
+        // the (PW-TX) x PH right columns: one position per thread, whole warps
+        static_assert((PW - TX) * PH == NT, "right columns of the staging tile: one per thread");
+        temps_at(tid / (PW - TX), TX + tid % (PW - TX));
         // this column's zz temporary and buoyancy at plane L
         const int kc = (ty + 8) * PW + tx + 8;
         float tz1, tz2;
@@ -737,7 +738,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
             }
         };
         dx_at(ty, tx);
-        if (tx < IW - TX) dx_at(ty, tx + TX);
+        if (tid < (IW - TX) * TY) dx_at(tid / (IW - TX), TX + tid % (IW - TX));
         dy_at(ty, tx);
         if (ty < IH - TY) dy_at(ty + TY, tx);
         // (3) D- z stage (compute_z_contributionsdtd), completes position L-3
@@ -1109,7 +1110,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             ays[IH * TX + r * TX + c] = t2.y;
         };
         xt_at(ty, tx);
-        if (tx < IW - TX) xt_at(ty, tx + TX);
+        if (tid < (IW - TX) * TY) xt_at(tid / (IW - TX), TX + tid % (IW - TX));
         yt_at(ty, tx);
         if (ty < IH - TY) yt_at(ty + TY, tx);
         // (2) column values: z temporaries, buoyancy, D- z stage of the stored p/q
@@ -1426,7 +1427,7 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.src_index = s.src_index;
     a.src_term = s.src_term;
     a.L = L;
-    a.bz = pick_bz(L);
+    a.bz = s.bz > 0 ? std::min(s.bz, L.nz()) : choose_bz(L, KIND_FWD);
     a.fs = s.free_surface;
     a.dt = s.dt;
     a.invdx = 1.0 / s.dx;
@@ -1435,7 +1436,7 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.invdxdy = 1.0 / (4 * s.dx * s.dy);
     a.invdydz = 1.0 / (4 * s.dy * s.dz);
     a.invdzdx = 1.0 / (4 * s.dx * s.dz);
-    a.err = err_word();
+    a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
     dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
     if (!kernels_prepared()) return TTI_ELAUNCH;
@@ -1465,7 +1466,7 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     a.aby = s.aby;
     a.abz = s.abz;
     a.L = L;
-    a.bz = pick_bz(L);
+    a.bz = s.bz > 0 ? std::min(s.bz, L.nz()) : choose_bz(L, KIND_ADJ);
     a.fs = s.free_surface;
     a.sponge = s.sponge_active;
     a.dt = s.dt;
@@ -1475,7 +1476,7 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     a.invdxy = 1.0 / (4 * s.dx * s.dy);
     a.invdyz = 1.0 / (4 * s.dy * s.dz);
     a.invdzx = 1.0 / (4 * s.dx * s.dz);
-    a.err = err_word();
+    a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
     const bool tti = !s.vti;
     dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
@@ -1555,13 +1556,13 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     a.gvp = s.grad_vp;
     a.grho = s.grad_rho;
     a.L = L;
-    a.bz = pick_bz(L);
+    a.bz = s.bz > 0 ? std::min(s.bz, L.nz()) : choose_bz(L, KIND_IMG);
     a.fs = s.free_surface;
     a.slot = s.slot;
     a.hx = 1.0 / s.dx;
     a.hy = 1.0 / s.dy;
     a.hz = 1.0 / s.dz;
-    a.err = err_word();
+    a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
     dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
     const bool tti = !s.vti;
@@ -1578,11 +1579,59 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
 
 int prepare_fused_kernels() { return kernels_prepared() ? TTI_OK : TTI_ELAUNCH; }
 
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_tuned;  // (device, nx, ny, nz, kind) -> bz
+int current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
+    return dev;
+}
+} // namespace
+
+void record_tuned_bz(const Layout& L, int kind, int bz)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    const auto key = std::make_tuple(current_device(), L.nx(), L.ny(), L.nz(), kind);
+    if (bz > 0)
+        g_tuned[key] = std::min(bz, L.nz());
+    else
+        g_tuned.erase(key);
+}
+
+int tuned_bz(const Layout& L, int kind)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(std::make_tuple(current_device(), L.nx(), L.ny(), L.nz(), kind));
+    return it == g_tuned.end() ? 0 : it->second;
+}
+
+int model_bz(const Layout& L) { return pick_bz(L); }
+
+int choose_bz(const Layout& L, int kind)
+{
+    const int t = tuned_bz(L, kind);
+    return t > 0 ? t : pick_bz(L);
+}
+
+std::vector<int> bz_candidates(const Layout& L)
+{
+    std::vector<int> out;
+    const int nz = L.nz();
+    for (int nch = 1; nch <= nz; ++nch) {
+        const int bz = (nz + nch - 1) / nch;
+        if (bz < 8 && nch > 1) break;
+        if (out.empty() || out.back() != bz) out.push_back(bz);
+    }
+    return out;
+}
+
 // Bounded-wait status of the fused kernels on the current device: 0 if no
 // wait gave up since the last call; the word is cleared.
-int fused_wait_status(cudaStream_t st)
+int fused_wait_status(cudaStream_t st, int* word)
 {
-    int* w = err_word();
+    int* w = word ? word : err_word();
     if (!w) return TTI_ENOMEM;
     int h = 0;
     if (cudaMemcpyAsync(&h, w, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 #include "tti_common.cuh"
 
@@ -51,6 +52,8 @@ struct FwdStepArgs {
     int vti;            // 1: rx=ry=0, rz=1 are not read
     float dt;
     double dx, dy, dz;
+    int* err = nullptr;  // error word of the bounded waits (nullptr: the device's)
+    int bz = 0;          // z planes per CTA (0: tuned or modelled choice)
 };
 int launch_fused_forward(const Layout& L, const FwdStepArgs& a, cudaStream_t st);
 
@@ -70,6 +73,8 @@ struct AdjStepArgs {
     int vti;
     float dt;
     double dx, dy, dz;
+    int* err = nullptr;
+    int bz = 0;
 };
 int launch_fused_adjoint(const Layout& L, const AdjStepArgs& a, cudaStream_t st);
 
@@ -93,13 +98,28 @@ struct ImageArgs {
     int free_surface;
     int vti;
     double dx, dy, dz;
+    int* err = nullptr;
+    int bz = 0;
 };
 bool fused_image_supported(const Layout& L);
 int launch_fused_image(const Layout& L, const ImageArgs& a, cudaStream_t st);
 
 // Status of the bounded waits inside the fused kernels since the last call
-// (TTI_ETIMEOUT if any gave up); synchronizes the stream.
-int fused_wait_status(cudaStream_t st);
+// (TTI_ETIMEOUT if any gave up, TTI_ERANGE if a reduced-precision snapshot
+// saturated); synchronizes the stream and clears the word.  word = nullptr
+// reads the device's shared word.
+int fused_wait_status(cudaStream_t st, int* word = nullptr);
+
+// z planes per CTA of a fused kernel (kind 0 forward, 1 adjoint, 2 imaging)
+// on this grid: the autotuned value if one was recorded, else the wave-count
+// model.
+enum { KIND_FWD = 0, KIND_ADJ = 1, KIND_IMG = 2 };
+int choose_bz(const Layout& L, int kind);
+void record_tuned_bz(const Layout& L, int kind, int bz);
+int tuned_bz(const Layout& L, int kind);  // 0 if none recorded
+int model_bz(const Layout& L);            // the wave-count model's choice
+// Candidate z-chunk lengths the tuner tries (each ceil(nz/n) >= 8, or nz).
+std::vector<int> bz_candidates(const Layout& L);
 
 // Sets the fused kernels' attributes and allocates the error word on the
 // current device (done by the first launch otherwise); call before a stream

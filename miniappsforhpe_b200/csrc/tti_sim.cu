@@ -24,6 +24,7 @@
 
 #include "tti_common.cuh"
 #include "tti_internal.cuh"
+#include "tti_shot.cuh"
 
 using namespace tti;
 
@@ -194,6 +195,7 @@ struct tti_sim {
     unsigned int* ckpt_amax = nullptr;  // running snapshot max at each checkpoint
     int ckpt = 0, ncp = 0;
     float *grad_vp = nullptr, *grad_rho = nullptr;
+    int* err = nullptr;  // error word of this simulator's fused kernels
     int64_t src_index = -1;
     std::vector<float> wavelet;
     int nrec = 0;
@@ -214,12 +216,17 @@ struct tti_sim {
     int64_t kind_n[3] = {0, 0, 0};
     int64_t launches = 0;
     int64_t ninterior = 0;
+    // resumable shot: phase 0 idle, 1 forward, 2 adjoint, 3 done
+    int sh_phase = 0, sh_n = 0, sh_seg = 0;
+    bool sh_recomp = false;
 
     int alloc(void** p, size_t bytes)
     {
         *p = nullptr;
         if (bytes == 0) return TTI_OK;
-        cudaError_t e = cudaMalloc(p, bytes);
+        // stream-ordered: creating and destroying simulators never
+        // synchronizes the device
+        cudaError_t e = cudaMallocAsync(p, bytes, stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             *p = nullptr;
@@ -277,7 +284,7 @@ Plan plan_of(const tti_sim_config& c)
     const size_t vb = (size_t)L.ldimx * L.ldimy * L.ldimz * sizeof(float);
     const size_t nin = (size_t)c.nx * c.ny * c.nz;
     pl.core = 6 * vb + 8 * vb + 2 * nin * sizeof(float) + (size_t)c.nt * sizeof(float) +
-              (size_t)(L.ldimx + L.ldimy + L.ldimz) * sizeof(float2);
+              (size_t)(L.ldimx + L.ldimy + L.ldimz) * sizeof(float2) + sizeof(int);
     pl.need_aux = !c.fused || (c.save_snapshots && !fused_image_supported(L));
     if (pl.need_aux) pl.aux = 10 * vb + 4 * vb;  // rhs3, rhs4, snp, snq, six derivatives, 4-float scratch
     if (c.save_snapshots) {
@@ -295,18 +302,18 @@ Plan plan_of(const tti_sim_config& c)
     return pl;
 }
 
-int sim_zero(tti_sim* s, void* p, size_t bytes)
+int sim_zero(tti_sim* s, void* p, size_t bytes, cudaStream_t st = nullptr)
 {
-    if (cudaMemsetAsync(p, 0, bytes, s->stream) != cudaSuccess) return cuda_rc(cudaGetLastError());
+    if (cudaMemsetAsync(p, 0, bytes, st ? st : s->stream) != cudaSuccess) return cuda_rc(cudaGetLastError());
     return TTI_OK;
 }
 
-int zero_state(tti_sim* s, WaveState& w)
+int zero_state(tti_sim* s, WaveState& w, cudaStream_t st = nullptr)
 {
     const size_t vb = (size_t)s->nvol() * sizeof(float);
     int rc = TTI_OK;
     for (float* v : {w.p, w.q, w.pd, w.qd, w.p2, w.q2})
-        if (!rc && v) rc = sim_zero(s, v, vb);
+        if (!rc && v) rc = sim_zero(s, v, vb, st);
     return rc;
 }
 
@@ -548,6 +555,7 @@ int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t s
     a.dx = c.dx;
     a.dy = c.dy;
     a.dz = c.dz;
+    a.err = s->err;
     mark_begin(s, 0, st);
     int rc = launch_fused_forward(s->L, a, st);
     mark_end(s, st);
@@ -579,6 +587,7 @@ int fused_adjoint_step(tti_sim* s, cudaStream_t st)
     a.dx = c.dx;
     a.dy = c.dy;
     a.dz = c.dz;
+    a.err = s->err;
     mark_begin(s, 1, st);
     int rc = launch_fused_adjoint(s->L, a, st);
     mark_end(s, st);
@@ -612,6 +621,7 @@ int image_step(tti_sim* s, int slot, cudaStream_t st)
         ia.dx = c.dx;
         ia.dy = c.dy;
         ia.dz = c.dz;
+        ia.err = s->err;
         rc = launch_fused_image(s->L, ia, st);
         s->launches++;
     } else {
@@ -646,7 +656,7 @@ int restore_checkpoint(tti_sim* s, WaveState& w, int k, cudaStream_t st)
 {
     const int64_t n = s->ninterior;
     float* slot = s->ckpts + (size_t)k * 4 * n;
-    int rc = zero_state(s, w);
+    int rc = zero_state(s, w, st);
     if (rc) return rc;
     k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(w.p, slot, s->L);
     k_interior_copy<false><<<s->dense_grid(), 128, 0, st>>>(w.q, slot + n, s->L);
@@ -660,6 +670,33 @@ int restore_checkpoint(tti_sim* s, WaveState& w, int k, cudaStream_t st)
     if (cudaMemcpyAsync(s->snap_amax, s->ckpt_amax + 4 * k, 4 * sizeof(unsigned int), cudaMemcpyDeviceToDevice, st) !=
         cudaSuccess)
         return cuda_rc(cudaGetLastError());
+    return launch_status();
+}
+
+// One adjoint step n (reference order, simulator2SetUp.cu:654-782): source
+// trace, residual injection, the step, and imaging at snapshot steps from
+// store slot (n - seg_start) / xcorr_step.  observed: s->resid holds observed
+// traces and the residual is formed from the last forward's traces.
+int adjoint_unit(tti_sim* s, int n, int seg_start, bool observed, cudaStream_t st)
+{
+    const tti_sim_config& c = s->cfg;
+    int r = TTI_OK;
+    if (s->src_index >= 0) {
+        k_source_trace<<<1, 1, 0, st>>>(s->srctr + n, s->w.p, s->w.q, s->src_index);
+        s->launches++;
+    }
+    if (s->nrec) {
+        const float* obs = observed ? s->resid + (size_t)n * s->nrec : nullptr;
+        const float* res = observed ? s->traces + (size_t)n * s->nrec : s->resid + (size_t)n * s->nrec;
+        k_inject_residual<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->w.pd, s->w.qd, s->rec, res, obs, s->nrec);
+        s->launches++;
+    }
+    if (!c.fused) {
+        if ((r = adjoint_per_kernel_step(s, st))) return r;
+    } else {
+        if ((r = fused_adjoint_step(s, st))) return r;
+    }
+    if (n % c.xcorr_step == 0 && (r = image_step(s, (n - seg_start) / c.xcorr_step, st))) return r;
     return launch_status();
 }
 
@@ -745,6 +782,8 @@ int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
             if (!rc) rc = s->alloc((void**)v, vb);
         if (!rc) rc = s->alloc((void**)&s->base, (size_t)s->nvol() * sizeof(float4));
     }
+    if (!rc) rc = s->alloc((void**)&s->err, sizeof(int));
+    if (!rc) rc = sim_zero(s, s->err, sizeof(int));
     if (!rc) rc = s->alloc((void**)&s->grad_vp, s->ninterior * sizeof(float));
     if (!rc) rc = s->alloc((void**)&s->grad_rho, s->ninterior * sizeof(float));
     if (!rc) rc = s->alloc((void**)&s->srctr, (size_t)c.nt * sizeof(float));
@@ -800,8 +839,12 @@ int tti_sim_destroy(tti_sim* s)
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     for (cudaGraphExec_t g : s->gexec)
         if (g) cudaGraphExecDestroy(g);
-    for (void* p : s->allocs) cudaFree(p);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    for (void* p : s->allocs)
+        if (p) cudaFreeAsync(p, s->stream);
+    if (s->stream) {
+        cudaStreamSynchronize(s->stream);
+        cudaStreamDestroy(s->stream);
+    }
     cudaGetLastError();
     delete s;
     return TTI_OK;
@@ -830,9 +873,9 @@ int tti_sim_set_model(tti_sim* s, const float* vp, const float* eps, const float
     float* dense = nullptr;
     float* par[7] = {};
     int rc = TTI_OK;
-    if (cudaMalloc(&dense, n * sizeof(float)) != cudaSuccess) return cuda_rc(cudaGetLastError());
+    if (cudaMallocAsync(&dense, n * sizeof(float), st) != cudaSuccess) return cuda_rc(cudaGetLastError());
     for (int k = 0; k < 7 && !rc; ++k) {
-        if (cudaMalloc(&par[k], s->nvol() * sizeof(float)) != cudaSuccess) {
+        if (cudaMallocAsync(&par[k], s->nvol() * sizeof(float), st) != cudaSuccess) {
             rc = cuda_rc(cudaGetLastError());
             break;
         }
@@ -859,9 +902,11 @@ int tti_sim_set_model(tti_sim* s, const float* vp, const float* eps, const float
         }
         if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
     }
-    cudaStreamSynchronize(st);
-    cudaFree(dense);
-    for (float* p : par) cudaFree(p);
+    cudaFreeAsync(dense, st);
+    for (float* p : par)
+        if (p) cudaFreeAsync(p, st);
+    if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
+    else cudaStreamSynchronize(st);
     if (!rc) s->model_set = true;
     return rc;
 }
@@ -890,7 +935,7 @@ int tti_sim_set_receivers(tti_sim* s, int nrec, const int* ixyz)
         if (sorted[r] == sorted[r - 1]) return TTI_EINVAL;
     for (void** p : {(void**)&s->rec, (void**)&s->traces, (void**)&s->resid}) {
         if (*p) {
-            cudaFree(*p);
+            cudaFreeAsync(*p, s->stream);
             for (auto& a : s->allocs)
                 if (a == *p) a = nullptr;
             *p = nullptr;
@@ -956,7 +1001,7 @@ int tti_sim_forward(tti_sim* s, float* traces, int traces_on_device)
         return rc;
     }
     rc = cuda_rc(cudaStreamSynchronize(s->stream));
-    if (!rc && fused) rc = fused_wait_status(s->stream);
+    if (!rc && fused) rc = fused_wait_status(s->stream, s->err);
     collect_marks(s);
     if (!rc) s->forward_done = true;
     return rc;
@@ -996,25 +1041,9 @@ static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device
     }
     const bool fused = c.fused != 0;
     auto adjoint_steps = [&](int hi, int lo, int seg_start, cudaStream_t st) -> int {
-        int r = TTI_OK;
         for (int n = hi; n >= lo; --n) {
-            if (s->src_index >= 0) {
-                k_source_trace<<<1, 1, 0, st>>>(s->srctr + n, s->w.p, s->w.q, s->src_index);
-                s->launches++;
-            }
-            if (s->nrec) {
-                const float* obs = observed ? s->resid + (size_t)n * s->nrec : nullptr;
-                const float* res = observed ? s->traces + (size_t)n * s->nrec : s->resid + (size_t)n * s->nrec;
-                k_inject_residual<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->w.pd, s->w.qd, s->rec, res, obs, s->nrec);
-                s->launches++;
-            }
-            if (!fused) {
-                if ((r = adjoint_per_kernel_step(s, st))) return r;
-            } else {
-                if ((r = fused_adjoint_step(s, st))) return r;
-            }
-            if (n % c.xcorr_step == 0 && (r = image_step(s, (n - seg_start) / c.xcorr_step, st))) return r;
-            if ((r = launch_status())) return r;
+            int r = adjoint_unit(s, n, seg_start, observed, st);
+            if (r) return r;
         }
         return TTI_OK;
     };
@@ -1046,10 +1075,151 @@ static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device
     k_finalize_dense<<<s->dense_grid(), 128, 0, st0>>>(s->grad_vp, s->mv[3], s->L, c.dt * c.xcorr_step);
     s->launches++;
     rc = cuda_rc(cudaStreamSynchronize(st0));
-    if (!rc && fused) rc = fused_wait_status(st0);
+    if (!rc && fused) rc = fused_wait_status(st0, s->err);
     collect_marks(s);
     return rc;
 }
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// A whole shot (forward with receivers, adjoint driven by observed traces,
+// imaging, finalisation) as a sequence of work units that can be enqueued a
+// few at a time on any stream, or captured.  A unit is one fused step:
+// forward, recomputed forward (checkpointed stores) or adjoint (with its
+// imaging).  Same kernels and order as tti_sim_forward followed by
+// tti_sim_adjoint_observed.
+namespace tti {
+
+int shot_upload_observed(tti_sim* s, const float* host_obs)
+{
+    if (!s) return TTI_EINVAL;
+    if (!s->nrec) return TTI_OK;
+    const size_t bytes = (size_t)s->nrec * s->cfg.nt * sizeof(float);
+    if (!host_obs) return sim_zero(s, s->resid, bytes);
+    if (cudaMemcpyAsync(s->resid, host_obs, bytes, cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+        return cuda_rc(cudaGetLastError());
+    return TTI_OK;
+}
+
+int shot_begin(tti_sim* s)
+{
+    if (!s) return TTI_EINVAL;
+    if (!s->cfg.fused || !s->cfg.save_snapshots) return TTI_EINVAL;
+    if (!s->model_set) return TTI_ESTATE;
+    s->launches = 0;
+    s->forward_done = false;
+    int rc = zero_state(s, s->w);
+    if (!rc && s->snap_amax) rc = sim_zero(s, s->snap_amax, 4 * sizeof(unsigned int));
+    if (rc) return rc;
+    s->sh_phase = 1;
+    s->sh_n = 0;
+    s->sh_seg = 0;
+    s->sh_recomp = false;
+    return TTI_OK;
+}
+
+int64_t shot_units_left(const tti_sim* s)
+{
+    if (!s || s->sh_phase == 0 || s->sh_phase == 3) return 0;
+    const int nt = s->cfg.nt, K = s->ckpt ? s->ckpt : nt;
+    const int last_a = ((nt - 1) / K) * K;  // start of the last segment
+    if (s->sh_phase == 1) return (int64_t)(nt - s->sh_n) + nt + last_a;
+    // adjoint: the rest of this segment, then the earlier segments in full
+    const int a = s->sh_seg * K;
+    int64_t left = s->sh_recomp ? (int64_t)(std::min(nt, a + K) - s->sh_n) + std::min(nt, a + K) - a
+                                : (int64_t)(s->sh_n - a + 1);
+    left += 2LL * a;  // segments 0 .. sh_seg-1: recompute + adjoint
+    return left;
+}
+
+bool shot_done(const tti_sim* s) { return s && s->sh_phase == 3; }
+
+cudaStream_t shot_stream(const tti_sim* s) { return s ? s->stream : nullptr; }
+
+// Enqueue up to max_units units on st.
+int shot_advance(tti_sim* s, cudaStream_t st, int64_t max_units, int64_t* done)
+{
+    if (!s || !done) return TTI_EINVAL;
+    *done = 0;
+    const tti_sim_config& c = s->cfg;
+    const int nt = c.nt, K = s->ckpt ? s->ckpt : nt;
+    const int nseg = (nt - 1) / K + 1;
+    int rc = TTI_OK;
+    while (*done < max_units && (s->sh_phase == 1 || s->sh_phase == 2)) {
+        if (s->sh_phase == 1) {
+            const int n = s->sh_n;
+            if (n == 0 && (rc = fused_prologue(s, s->w, st))) return rc;
+            if (s->ckpt && n % s->ckpt == 0 && (rc = save_checkpoint(s, s->w, n / s->ckpt, st))) return rc;
+            const int slot = (n % c.xcorr_step == 0) ? (s->ckpt ? (n % s->ckpt) / c.xcorr_step : n / c.xcorr_step) : -1;
+            if ((rc = receivers_step(s, s->w, n, st))) return rc;
+            if ((rc = fused_forward_step(s, s->w, n, slot, st))) return rc;
+            ++*done;
+            if (++s->sh_n == nt) {  // into the adjoint: last segment first, its snapshots are in the store
+                if ((rc = zero_state(s, s->w, st))) return rc;
+                if ((rc = sim_zero(s, s->grad_vp, s->ninterior * sizeof(float), st))) return rc;
+                if ((rc = sim_zero(s, s->grad_rho, s->ninterior * sizeof(float), st))) return rc;
+                s->sh_phase = 2;
+                s->sh_seg = nseg - 1;
+                s->sh_recomp = false;
+                s->sh_n = nt - 1;
+            }
+        } else {
+            const int a = s->sh_seg * K, b = std::min(nt, a + K);
+            if (s->sh_recomp) {
+                const int n = s->sh_n;
+                if (n == a && (rc = restore_checkpoint(s, s->rw, s->sh_seg, st))) return rc;
+                const int slot = (n % c.xcorr_step == 0) ? (n - a) / c.xcorr_step : -1;
+                if ((rc = fused_forward_step(s, s->rw, n, slot, st))) return rc;
+                ++*done;
+                if (++s->sh_n == b) {
+                    s->sh_recomp = false;
+                    s->sh_n = b - 1;
+                }
+            } else {
+                if ((rc = adjoint_unit(s, s->sh_n, a, true, st))) return rc;
+                ++*done;
+                if (--s->sh_n < a) {
+                    if (--s->sh_seg < 0) {
+                        k_finalize_dense<<<s->dense_grid(), 128, 0, st>>>(s->grad_vp, s->mv[3], s->L,
+                                                                         c.dt * c.xcorr_step);
+                        s->launches++;
+                        s->sh_phase = 3;
+                    } else {
+                        s->sh_recomp = true;
+                        s->sh_n = s->sh_seg * K;
+                    }
+                }
+            }
+        }
+        if ((rc = launch_status())) return rc;
+    }
+    return TTI_OK;
+}
+
+int shot_read_traces(tti_sim* s, float* host)
+{
+    if (!s || !host) return TTI_EINVAL;
+    if (!s->nrec) return TTI_OK;
+    const size_t bytes = (size_t)s->nrec * s->cfg.nt * sizeof(float);
+    if (cudaMemcpyAsync(host, s->traces, bytes, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+        return cuda_rc(cudaGetLastError());
+    return cuda_rc(cudaStreamSynchronize(s->stream));
+}
+
+// After the enqueued units have run: status of the shot's kernels.
+int shot_end(tti_sim* s)
+{
+    if (!s) return TTI_EINVAL;
+    int rc = cuda_rc(cudaStreamSynchronize(s->stream));
+    if (!rc) rc = fused_wait_status(s->stream, s->err);
+    if (!rc && s->sh_phase == 3) s->forward_done = true;
+    return rc;
+}
+
+} // namespace tti
+
+extern "C" {
 
 int tti_sim_get_image(tti_sim* s, float* grad_vp, float* grad_rho, int on_device)
 {
@@ -1082,6 +1252,154 @@ int tti_sim_kernel_times(tti_sim* s, double* ms, int64_t* launches)
         launches[k] = s->kind_n[k];
     }
     return TTI_OK;
+}
+
+int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
+{
+    if (!s || !out || reps < 1) return TTI_EINVAL;
+    if (!s->cfg.fused) return TTI_EINVAL;
+    if (!s->model_set) return TTI_ESTATE;
+    *out = tti_tune_report{};
+    const Layout& L = s->L;
+    const tti_sim_config& c = s->cfg;
+    const bool img = s->snaps && (c.snap_precision != SNAP_F32 || fused_image_supported(L));
+    const std::vector<int> cand = bz_candidates(L);
+    out->ncand = (int)cand.size();
+    cudaStream_t st = s->stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        cudaGetLastError();
+        return TTI_ELAUNCH;
+    }
+    // Each candidate runs on the simulator's own volumes; the wavefield and
+    // image contents afterwards are unspecified (forward() and adjoint()
+    // start from zero).
+    auto launch = [&](int kind, int bz) -> int {
+        WaveState& w = s->w;
+        if (kind == KIND_FWD) {
+            FwdStepArgs a{};
+            a.pin = w.p;
+            a.qin = w.q;
+            a.pout = w.p2;
+            a.qout = w.q2;
+            a.f3 = w.pd;
+            a.f4 = w.qd;
+            a.m = model_of(s);
+            a.abx = s->abx;
+            a.aby = s->aby;
+            a.abz = s->abz;
+            a.src_index = -1;
+            a.snap_prec = c.snap_precision;
+            a.free_surface = c.free_surface;
+            a.vti = s->vti ? 1 : 0;
+            a.dt = c.dt;
+            a.dx = c.dx;
+            a.dy = c.dy;
+            a.dz = c.dz;
+            a.err = s->err;
+            a.bz = bz;
+            return launch_fused_forward(L, a, st);
+        }
+        if (kind == KIND_ADJ) {
+            AdjStepArgs a{};
+            a.pin = w.p;
+            a.qin = w.q;
+            a.pout = w.p2;
+            a.qout = w.q2;
+            a.f3 = w.pd;
+            a.f4 = w.qd;
+            a.m = model_of(s);
+            a.abx = s->abx;
+            a.aby = s->aby;
+            a.abz = s->abz;
+            a.sponge_active = s->sponge_active ? 1 : 0;
+            a.free_surface = c.free_surface;
+            a.vti = s->vti ? 1 : 0;
+            a.dt = c.dt;
+            a.dx = c.dx;
+            a.dy = c.dy;
+            a.dz = c.dz;
+            a.err = s->err;
+            a.bz = bz;
+            return launch_fused_adjoint(L, a, st);
+        }
+        ImageArgs ia{};
+        ia.adj1 = w.p;
+        ia.adj2 = w.q;
+        ia.adj3 = w.pd;
+        ia.adj4 = w.qd;
+        ia.store = s->snaps;
+        ia.snap_prec = c.snap_precision;
+        ia.snap_scale = s->snap_scale;
+        ia.nsnap = s->nslot;
+        ia.slot = 0;
+        ia.m = model_of(s);
+        ia.grad_vp = s->grad_vp;
+        ia.grad_rho = s->grad_rho;
+        ia.free_surface = c.free_surface;
+        ia.vti = s->vti ? 1 : 0;
+        ia.dx = c.dx;
+        ia.dy = c.dy;
+        ia.dz = c.dz;
+        ia.err = s->err;
+        ia.bz = bz;
+        return launch_fused_image(L, ia, st);
+    };
+    int rc = TTI_OK;
+    if (s->snap_scale) rc = sim_zero(s, s->snap_scale, (size_t)s->nslot * 4 * sizeof(float));
+    for (int kind = 0; kind < 3 && !rc; ++kind) {
+        if (kind == KIND_IMG && !img) continue;
+        float best = 1e30f;
+        int best_bz = 0;
+        for (int bz : cand) {
+            if ((rc = launch(kind, bz))) break;  // warm-up
+            cudaEventRecord(e0, st);
+            for (int r = 0; r < reps && !rc; ++r) rc = launch(kind, bz);
+            cudaEventRecord(e1, st);
+            if (rc) break;
+            if ((rc = cuda_rc(cudaEventSynchronize(e1)))) break;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= reps;
+            if (bz == model_bz(L)) out->model_ms[kind] = ms;
+            if (ms < best) {
+                best = ms;
+                best_bz = bz;
+            }
+        }
+        if (rc) break;
+        record_tuned_bz(L, kind, best_bz);
+        out->bz[kind] = best_bz;
+        out->ms[kind] = best;
+    }
+    if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
+    if (!rc) rc = fused_wait_status(st, s->err);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGetLastError();
+    return rc;
+}
+
+int tti_tune_set(int nx, int ny, int nz, int kind, int bz)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind > 2 || bz < 0) return TTI_EINVAL;
+    tti_sim_config c{};
+    c.nx = nx;
+    c.ny = ny;
+    c.nz = nz;
+    record_tuned_bz(layout_of(c), kind, bz);
+    return TTI_OK;
+}
+
+int tti_tune_get(int nx, int ny, int nz, int kind)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind > 2) return -TTI_EINVAL;
+    tti_sim_config c{};
+    c.nx = nx;
+    c.ny = ny;
+    c.nz = nz;
+    return choose_bz(layout_of(c), kind);
 }
 
 int tti_sim_source_gradient(tti_sim* s, float* host_out)
