@@ -34,6 +34,7 @@ METRIC = "TTI fwd+adj+grad Gpts/s & HBM % of peak; shots/hr, p50/p99 at fixed im
 # forward TTI 64, adjoint TTI 64, imaging 16 per imaging step, snapshot 8 per
 # snapshot step; the fused kernels' per-launch figure is 64 B/pt.
 B_FWD, B_ADJ, B_IMG, B_SNAP = 64, 64, 16, 8
+B_VTI = 52  # forward or adjoint step on a VTI model: rx, ry, rz are not read
 
 
 def parse():
@@ -320,7 +321,9 @@ def run_ours(args):
     kind = max(("forward", "adjoint"), key=lambda k: times[k][0])
     kms, kn = times[kind]
     per_launch_s = (kms / max(kn, 1)) / 1e3
-    alg_bytes = (B_FWD if kind == "forward" else B_ADJ) * npts
+    vti = args.model == "layered"
+    b_step = B_VTI if vti else (B_FWD if kind == "forward" else B_ADJ)
+    alg_bytes = b_step * npts
     achieved = alg_bytes / per_launch_s / 1e9 if kn else None
     traffic = ncu_traffic().get(f"{kind}_dram_bytes_per_launch_{nx}x{ny}x{nz}")
     roofline = {"kernel": f"fused {kind} step", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -329,7 +332,7 @@ def run_ours(args):
                 "avg_launch_ms": per_launch_s * 1e3, "launches": kn}
     passes = {k: {"total_ms": v[0] / args.steps, "launches_per_shot": v[1] / args.steps}
               for k, v in times.items()}
-    step_bytes = (B_FWD + B_ADJ + B_IMG / args.xcorr + B_SNAP / args.xcorr) * npts
+    step_bytes = ((2 * B_VTI if vti else B_FWD + B_ADJ) + B_IMG / args.xcorr + B_SNAP / args.xcorr) * npts
     hbm_frac = step_bytes * args.nt / (ms_per_step / 1e3) / 1e9 / peak
 
     # end to end through the host-buffer API
@@ -371,7 +374,7 @@ def run_ours(args):
         "config": {**desc, "parallelism": f"shot-parallel x{ws}" if ws > 1 else "single GPU",
                    "path": "reference kernel sequence" if args.per_kernel else "fused step kernels",
                    "snapshots": args.snap_precision},
-        "roofline": roofline, "hbm_frac_alg_134B": hbm_frac,
+        "roofline": roofline, "hbm_frac_alg_per_step": hbm_frac,
         "shots_per_hour": 3600.0 * 1e3 / ms_per_step * ws,
         "passes_ms_per_shot": passes, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clocks,

@@ -249,15 +249,19 @@ int tti_sim_adjoint(tti_sim* sim, const float* residual, int residual_on_device)
  * traces of the last forward run minus these observed traces (nt*nrec). */
 int tti_sim_adjoint_observed(tti_sim* sim, const float* observed, int observed_on_device);
 
-/* z-chunk autotuner.  The fused kernels run one CTA per SM on a
- * TX x TY x bz block of outputs (TX = 32, TY = 16) marching along z; bz sets
- * how many CTAs a step launches against the pipeline fill of each chunk.
- * tti_sim_autotune times every candidate bz (ceil(nz/n) >= 8) of the fused
+/* z-chunk autotuner.  The fused kernels run one CTA per SM on TX x TY
+ * column tiles (TX = 32, TY = 16) marching along z; the grid's planes are
+ * split among CTAs in tile-major order, bz consecutive planes per CTA (one
+ * or more column segments, each paying a pipeline fill of 14 planes), so bz
+ * sets how many CTAs a step launches against the fill overhead.
+ * tti_sim_autotune times every candidate bz (whole-column chunks ceil(nz/n)
+ * and equal shares for 1..8 CTAs per SM, at least 8 planes) of the fused
  * forward, adjoint and (with a snapshot store) imaging kernels on this
  * simulator's volumes, reps launches each, and records the fastest for this
  * grid on the current device; later launches on any simulator of the same
  * grid use it.  Needs fused = 1 and a model.  Wavefield and image contents
- * afterwards are unspecified (forward and adjoint start from zero). */
+ * afterwards are unspecified (forward and adjoint start from zero).  The
+ * split changes only the launch shape: results do not depend on bz. */
 typedef struct {
     int bz[3];         /* chosen bz: forward, adjoint, imaging (0: not tuned) */
     float ms[3];       /* per-launch time at the chosen bz */
@@ -266,7 +270,7 @@ typedef struct {
 } tti_tune_report;
 int tti_sim_autotune(tti_sim* sim, int reps, tti_tune_report* out);
 
-/* Record (bz > 0) or clear (bz = 0) the z-chunk used for kernel kind
+/* Record (bz > 0) or clear (bz = 0) the planes per CTA used for kernel kind
  * (0 forward, 1 adjoint, 2 imaging) on an nx*ny*nz grid, current device;
  * tti_tune_get returns the bz in effect (recorded or modelled). */
 int tti_tune_set(int nx, int ny, int nz, int kind, int bz);

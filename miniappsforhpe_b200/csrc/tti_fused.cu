@@ -99,6 +99,45 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 }
 
 // ---------------------------------------------------------------------------
+// Work split of one fused step.  The grid's (tile, z) planes are taken in
+// tile-major order (all of tile 0's column, then tile 1's, ...) and every CTA
+// processes per_cta consecutive planes of that sequence, as one or more
+// segments that each lie in one tile column.  A segment costs its planes
+// plus the 2*LAG planes of pipeline fill, so per_cta is chosen to balance
+// the SMs rather than to cut columns evenly.
+struct Segment {
+    int x0, y0, zs, len;
+};
+struct WorkRange {
+    long long pos, end;
+    int tiles_x, nz, ixbeg, iybeg, izbeg;
+    __device__ WorkRange(const Layout& L, int per_cta)
+    {
+        tiles_x = (L.nx() + TX - 1) / TX;
+        const int tiles_y = (L.ny() + TY - 1) / TY;
+        nz = L.nz();
+        ixbeg = L.ixbeg;
+        iybeg = L.iybeg;
+        izbeg = L.izbeg;
+        const long long W = (long long)tiles_x * tiles_y * nz;
+        pos = (long long)blockIdx.x * per_cta;
+        end = min(W, pos + per_cta);
+    }
+    __device__ bool next(Segment& sg)
+    {
+        if (pos >= end) return false;
+        const long long tile = pos / nz;
+        const int z0 = (int)(pos - tile * nz);
+        sg.len = (int)min((long long)(nz - z0), end - pos);
+        sg.x0 = ixbeg + (int)(tile % tiles_x) * TX;
+        sg.y0 = iybeg + (int)(tile / tiles_x) * TY;
+        sg.zs = izbeg + z0;
+        pos += sg.len;
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------------------
 // Free-surface resolution of the buoyancy-scaled z-derivative queue.
 // q[j] holds the derivative at position z-3+j.  The z-marching pipeline
 // already zeroes positions outside the interior (the reference's derivative
@@ -176,22 +215,28 @@ __global__ void __launch_bounds__(NT, 1)
 
     const Layout& L = a.L;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int x0 = L.ixbeg + blockIdx.x * TX, y0 = L.iybeg + blockIdx.y * TY;
-    const int zs = L.izbeg + blockIdx.z * a.bz;
-    const int ze = min(zs + a.bz - 1, L.izend);
-    const int ntot = ze - zs + 1 + 2 * LAG;  // arrival planes zs-7 .. ze+7
-    const int x = x0 + tx, y = y0 + ty;
-    const bool owner = (x <= L.ixend) && (y <= L.iyend);
     bool dead = false;
 
     if (tid == 0) {
         for (int s = 0; s < FWD_NS; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
-    __syncthreads();
+    unsigned tmax[4] = {0u, 0u, 0u, 0u};  // max |stored value| seen by this thread
+    int s = 0;                            // ring slot of the current plane
+    uint32_t phase = 0;                   // mbarrier parity of slot s for this use
+    int gbase = 0;                        // planes consumed by earlier segments
+    // This CTA's share of the (tile, z) work in tile-major order: a.bz planes
+    // from blockIdx.x * a.bz, as one or more segments of a tile column.
+    WorkRange wr(L, a.bz);
+    for (Segment sg; wr.next(sg); gbase += sg.len + 2 * LAG) {
+    const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
+    const int ntot = sg.len + 2 * LAG;  // arrival planes zs-7 .. ze+7
+    const int x = x0 + tx, y = y0 + ty;
+    const bool owner = (x <= L.ixend) && (y <= L.iyend);
+    __syncthreads();  // barriers initialised; the previous segment is done with the ring
 
     auto issue = [&](int t) {
-        const int s = t % FWD_NS, z = zs - LAG + t;
+        const int s = (gbase + t) % FWD_NS, z = zs - LAG + t;
         float* dst = ring + (size_t)s * 2 * PH * PW;
         mbar_expect_tx(&bars[s], (uint32_t)(FWD_SLOT_P + FWD_SLOT_I));
         tma_load_3d(dst, &tm_p, x0 - 8, y0 - 8, z, &bars[s]);
@@ -212,10 +257,7 @@ __global__ void __launch_bounds__(NT, 1)
         for (int c = 0; c < 4; ++c) mq[j][c] = 0.0f;
 
     const int vc = (tx + 8), vr = (ty + 8);  // this column inside a p/q tile
-    unsigned tmax[4] = {0u, 0u, 0u, 0u};    // max |stored value| seen by this thread
 
-    int s = 0;           // ring slot of plane t
-    uint32_t phase = 0;  // mbarrier parity of slot s for this use
     auto back = [&](int k) { const int v = s - k; return v < 0 ? v + FWD_NS : v; };
     for (int t = 0; t < ntot; ++t) {
         __syncthreads();  // every thread is done with iteration t-1
@@ -473,7 +515,8 @@ __global__ void __launch_bounds__(NT, 1)
             phase ^= 1u;
         }
     }
-    // one atomic per warp and field for the whole z chunk; the next
+    }  // segments
+    // one atomic per warp and field for all segments; the next
     // snapshot's scale is taken from this running max
     if (a.snap && a.snap_prec != SNAP_F32) {
 #pragma unroll
@@ -577,12 +620,6 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
 
     const Layout& L = a.L;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int x0 = L.ixbeg + blockIdx.x * TX, y0 = L.iybeg + blockIdx.y * TY;
-    const int zs = L.izbeg + blockIdx.z * a.bz;
-    const int ze = min(zs + a.bz - 1, L.izend);
-    const int ntot = ze - zs + 1 + 2 * LAG;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool owner = (x <= L.ixend) && (y <= L.iyend);
     bool dead = false;
     constexpr int NLOAD = TTI ? ADJ_NARR : S_RX;  // VTI: rx, ry, rz are not read
     constexpr uint32_t TX_BYTES = (uint32_t)(NLOAD * ADJ_ARR + (TTI ? ADJ_RZ : 0));
@@ -591,10 +628,19 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
         for (int s = 0; s < ADJ_NSTAGE; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
-    __syncthreads();
+    int s = 0;
+    uint32_t phase = 0;
+    int gbase = 0;  // planes consumed by earlier segments
+    WorkRange wr(L, a.bz);
+    for (Segment sg; wr.next(sg); gbase += sg.len + 2 * LAG) {
+    const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
+    const int ntot = sg.len + 2 * LAG;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool owner = (x <= L.ixend) && (y <= L.iyend);
+    __syncthreads();  // barriers initialised; the previous segment is done with the stages
 
     auto issue = [&](int t) {
-        const int s = t % ADJ_NSTAGE, z = zs - LAG + t;
+        const int s = (gbase + t) % ADJ_NSTAGE, z = zs - LAG + t;
         float* dst = stage + (size_t)s * (ADJ_STAGE / sizeof(float));
         mbar_expect_tx(&bars[s], TX_BYTES);
 #pragma unroll
@@ -618,8 +664,6 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
 #pragma unroll
     for (int j = 0; j < 4; ++j) irq[j] = 0.0f;
 
-    int s = 0;
-    uint32_t phase = 0;
     for (int t = 0; t < ntot; ++t) {
         // Stage (t+2)%3 was last read in iteration t-1, before its final barrier.
         if (tid == 0 && t + ADJ_PF < ntot) {
@@ -892,6 +936,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
             phase ^= 1u;
         }
     }
+    }  // segments
 }
 
 // ---------------------------------------------------------------------------
@@ -977,13 +1022,6 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
 
     const Layout& L = a.L;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int x0 = L.ixbeg + blockIdx.x * TX, y0 = L.iybeg + blockIdx.y * TY;
-    const int xd0 = blockIdx.x * TX, yd0 = blockIdx.y * TY;  // dense (interior) origin
-    const int zs = L.izbeg + blockIdx.z * a.bz;
-    const int ze = min(zs + a.bz - 1, L.izend);
-    const int ntot = ze - zs + 1 + 2 * LAG;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool owner = (x <= L.ixend) && (y <= L.iyend);
     const int nx = L.nx(), ny = L.ny();
     bool dead = false;
     constexpr int NADJ = TTI ? IMG_NADJ : A_RX;
@@ -1001,12 +1039,23 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
         for (int s = 0; s < IMG_NSTAGE; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
-    __syncthreads();
+    int s = 0;
+    uint32_t phase = 0;
+    int gbase = 0;  // planes consumed by earlier segments
+    WorkRange wr(L, a.bz);
+    for (Segment sg; wr.next(sg); gbase += sg.len + 2 * LAG) {
+    const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
+    const int xd0 = x0 - L.ixbeg, yd0 = y0 - L.iybeg;  // dense (interior) origin
+    const int ze = zs + sg.len - 1;
+    const int ntot = sg.len + 2 * LAG;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool owner = (x <= L.ixend) && (y <= L.iyend);
+    __syncthreads();  // barriers initialised; the previous segment is done with the stages
 
     // plane z of the stored p/q: dense z = z - izbeg; above the surface the
     // free surface mirrors it (2*izbeg - z), without one it is zero halo.
     auto issue = [&](int t) {
-        const int s = t % IMG_NSTAGE, z = zs - LAG + t;
+        const int s = (gbase + t) % IMG_NSTAGE, z = zs - LAG + t;
         unsigned char* dst = stage + (size_t)s * IMG_STAGE;
         mbar_expect_tx(&bars[s], TX_BYTES);
         int zd = z - L.izbeg;
@@ -1030,8 +1079,6 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
 #pragma unroll
     for (int j = 0; j < 12; ++j) az1q[j] = az2q[j] = 0.0f;
 
-    int s = 0;
-    uint32_t phase = 0;
     for (int t = 0; t < ntot; ++t) {
         __syncthreads();  // the x/y tiles of plane L-1 have been read by every thread
         if (tid == 0 && t + IMG_PF < ntot) {
@@ -1229,6 +1276,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             phase ^= 1u;
         }
     }
+    }  // segments
 }
 
 // ---------------------------------------------------------------------------
@@ -1366,27 +1414,71 @@ bool layout_supported(const Layout& L)
            L.ldimz == L.izend + 1 + kRadius;
 }
 
-int pick_bz(const Layout& L)
+int device_sms()
 {
-    // One CTA per SM (shared memory bound).  Time ~ waves * (bz + 2*LAG):
-    // fewer, longer chunks amortise the 14-plane pipeline fill, more chunks
-    // fill the 148 SMs.
     int sms = 148;
-    {
-        int dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaGetLastError();
-    }
-    const long tiles = (long)((L.nx() + TX - 1) / TX) * ((L.ny() + TY - 1) / TY);
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    return sms;
+}
+
+long long work_planes(const Layout& L)
+{
+    return (long long)((L.nx() + TX - 1) / TX) * ((L.ny() + TY - 1) / TY) * L.nz();
+}
+
+// CTAs of a launch with bz planes per CTA.
+unsigned cta_count(const Layout& L, int bz) { return (unsigned)((work_planes(L) + bz - 1) / bz); }
+
+// Planes per CTA worth trying: whole-column chunks ceil(nz/n), and shares
+// that give every SM one, two, ... equal parts of the work; at least 8.
+std::vector<int> plane_candidates(const Layout& L)
+{
+    std::vector<int> c;
     const int nz = L.nz();
-    int best = nz;
-    double best_cost = 1e300;
     for (int nch = 1; nch <= nz; ++nch) {
         const int bz = (nz + nch - 1) / nch;
         if (bz < 8 && nch > 1) break;
-        const long ctas = tiles * ((nz + bz - 1) / bz);
-        const double waves = (double)((ctas + sms - 1) / sms);
-        const double cost = waves * (bz + 2 * LAG);
+        c.push_back(bz);
+    }
+    const long long W = work_planes(L);
+    const int sms = device_sms();
+    for (int k = 1; k <= 8; ++k) {
+        const long long b = (W + (long long)sms * k - 1) / ((long long)sms * k);
+        if (b >= 8 && b <= (1LL << 30)) c.push_back((int)b);
+    }
+    std::sort(c.begin(), c.end());
+    c.erase(std::unique(c.begin(), c.end()), c.end());
+    return c;
+}
+
+// Modelled time of a step, in plane-iterations of the slowest CTA: one CTA
+// per SM (shared memory bound), each segment pays the 2*LAG-plane pipeline
+// fill, a range of bz planes covers at most ceil((bz-1)/nz)+1 columns (one
+// when whole columns divide evenly).
+double plane_cost(const Layout& L, int bz)
+{
+    const int nz = L.nz();
+    const long long ctas = cta_count(L, bz);
+    const int sms = device_sms();
+    const double waves = (double)((ctas + sms - 1) / sms);
+    int segs;
+    if (bz <= nz && nz % bz == 0)
+        segs = 1;
+    else if (bz % nz == 0)
+        segs = bz / nz;
+    else
+        segs = (bz - 1) / nz + 2;
+    return waves * (bz + 2.0 * LAG * segs);
+}
+
+int pick_bz(const Layout& L)
+{
+    int best = L.nz();
+    double best_cost = 1e300;
+    for (int bz : plane_candidates(L)) {
+        const double cost = plane_cost(L, bz);
         if (cost < best_cost - 1e-9) {
             best_cost = cost;
             best = bz;
@@ -1427,7 +1519,7 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.src_index = s.src_index;
     a.src_term = s.src_term;
     a.L = L;
-    a.bz = s.bz > 0 ? std::min(s.bz, L.nz()) : choose_bz(L, KIND_FWD);
+    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_FWD);
     a.fs = s.free_surface;
     a.dt = s.dt;
     a.invdx = 1.0 / s.dx;
@@ -1438,7 +1530,7 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.invdzdx = 1.0 / (4 * s.dx * s.dz);
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
-    dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
+    dim3 grid(cta_count(L, a.bz));
     if (!kernels_prepared()) return TTI_ELAUNCH;
     if (s.vti)
         k_fused_forward<false><<<grid, dim3(TX, TY), FWD_SMEM, st>>>(mp, mq, mi, a);
@@ -1466,7 +1558,7 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     a.aby = s.aby;
     a.abz = s.abz;
     a.L = L;
-    a.bz = s.bz > 0 ? std::min(s.bz, L.nz()) : choose_bz(L, KIND_ADJ);
+    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_ADJ);
     a.fs = s.free_surface;
     a.sponge = s.sponge_active;
     a.dt = s.dt;
@@ -1479,7 +1571,7 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
     const bool tti = !s.vti;
-    dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
+    dim3 grid(cta_count(L, a.bz));
     if (!kernels_prepared()) return TTI_ELAUNCH;
     if (!tti)
         k_fused_adjoint<false><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
@@ -1556,7 +1648,7 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     a.gvp = s.grad_vp;
     a.grho = s.grad_rho;
     a.L = L;
-    a.bz = s.bz > 0 ? std::min(s.bz, L.nz()) : choose_bz(L, KIND_IMG);
+    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_IMG);
     a.fs = s.free_surface;
     a.slot = s.slot;
     a.hx = 1.0 / s.dx;
@@ -1564,7 +1656,7 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     a.hz = 1.0 / s.dz;
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
-    dim3 grid((L.nx() + TX - 1) / TX, (L.ny() + TY - 1) / TY, (L.nz() + a.bz - 1) / a.bz);
+    dim3 grid(cta_count(L, a.bz));
     const bool tti = !s.vti;
     if (!kernels_prepared()) return TTI_ELAUNCH;
     switch (s.snap_prec) {
@@ -1595,7 +1687,7 @@ void record_tuned_bz(const Layout& L, int kind, int bz)
     std::lock_guard<std::mutex> lk(g_tune_mu);
     const auto key = std::make_tuple(current_device(), L.nx(), L.ny(), L.nz(), kind);
     if (bz > 0)
-        g_tuned[key] = std::min(bz, L.nz());
+        g_tuned[key] = bz;
     else
         g_tuned.erase(key);
 }
@@ -1615,17 +1707,7 @@ int choose_bz(const Layout& L, int kind)
     return t > 0 ? t : pick_bz(L);
 }
 
-std::vector<int> bz_candidates(const Layout& L)
-{
-    std::vector<int> out;
-    const int nz = L.nz();
-    for (int nch = 1; nch <= nz; ++nch) {
-        const int bz = (nz + nch - 1) / nch;
-        if (bz < 8 && nch > 1) break;
-        if (out.empty() || out.back() != bz) out.push_back(bz);
-    }
-    return out;
-}
+std::vector<int> bz_candidates(const Layout& L) { return plane_candidates(L); }
 
 // Bounded-wait status of the fused kernels on the current device: 0 if no
 // wait gave up since the last call; the word is cleared.

@@ -53,7 +53,7 @@ struct FwdStepArgs {
     float dt;
     double dx, dy, dz;
     int* err = nullptr;  // error word of the bounded waits (nullptr: the device's)
-    int bz = 0;          // z planes per CTA (0: tuned or modelled choice)
+    int bz = 0;          // planes per CTA of the tile-major (tile, z) work (0: tuned or modelled)
 };
 int launch_fused_forward(const Layout& L, const FwdStepArgs& a, cudaStream_t st);
 
@@ -110,15 +110,17 @@ int launch_fused_image(const Layout& L, const ImageArgs& a, cudaStream_t st);
 // reads the device's shared word.
 int fused_wait_status(cudaStream_t st, int* word = nullptr);
 
-// z planes per CTA of a fused kernel (kind 0 forward, 1 adjoint, 2 imaging)
-// on this grid: the autotuned value if one was recorded, else the wave-count
-// model.
+// Planes per CTA of a fused kernel (kind 0 forward, 1 adjoint, 2 imaging) on
+// this grid: each CTA takes that many consecutive planes of the grid's
+// (tile, z) planes in tile-major order.  The autotuned value if one was
+// recorded, else the wave-count model's.
 enum { KIND_FWD = 0, KIND_ADJ = 1, KIND_IMG = 2 };
 int choose_bz(const Layout& L, int kind);
 void record_tuned_bz(const Layout& L, int kind, int bz);
 int tuned_bz(const Layout& L, int kind);  // 0 if none recorded
 int model_bz(const Layout& L);            // the wave-count model's choice
-// Candidate z-chunk lengths the tuner tries (each ceil(nz/n) >= 8, or nz).
+// Candidates the tuner tries: whole-column chunks ceil(nz/n) and equal
+// shares of the work for 1..8 CTAs per SM, each at least 8 planes.
 std::vector<int> bz_candidates(const Layout& L);
 
 // Sets the fused kernels' attributes and allocates the error word on the

@@ -6,9 +6,10 @@
 // simulator's own stream and hands it to the scheduler.  The scheduler runs
 // rounds: every resident shot's next units (fused steps) go into one launch
 // as parallel branches forked from and joined back into the server's stream,
-// captured as a CUDA graph when use_graphs is set.  Round r+1 is planned and
-// captured while round r runs; shots that finish in round r are read back and
-// released after it completes, while round r+1 runs.
+// captured as a CUDA graph when use_graphs is set.  Round r+1 is planned,
+// captured and issued behind round r while r runs, so the device does not
+// wait for the host between rounds; shots that finish in round r are read
+// back and released after it completes, while round r+1 runs.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -340,9 +341,19 @@ void scheduler_main(tti_server* srv)
             s->planned_left -= u;
             if (s->planned_left == 0) finishing.push_back(s);
         }
+        // issue round r+1 behind the round in flight, so the device never
+        // waits for the host between rounds
         int rc = TTI_OK;
-        if (!plan.empty()) rc = build_round(srv, plan, slot);
-        // wait for the round in flight, then retire what it finished
+        if (!plan.empty()) {
+            rc = build_round(srv, plan, slot);
+            if (!rc && srv->cfg.use_graphs) {
+                cudaEventRecord(srv->round_start[slot], srv->main);
+                rc = rc_of(cudaGraphLaunch(srv->exec[slot], srv->main));
+            }
+            if (!rc) rc = rc_of(cudaEventRecord(srv->round_end[slot], srv->main));
+        }
+        // then wait for the round in flight and retire what it finished,
+        // while round r+1 runs
         if (inflight) {
             cudaEventSynchronize(srv->round_end[slot ^ 1]);
             float ms = 0;
@@ -359,13 +370,6 @@ void scheduler_main(tti_server* srv)
             inflight = false;
         }
         if (plan.empty()) continue;
-        if (!rc) {
-            if (srv->cfg.use_graphs) {
-                cudaEventRecord(srv->round_start[slot], srv->main);
-                rc = rc_of(cudaGraphLaunch(srv->exec[slot], srv->main));
-            }
-            cudaEventRecord(srv->round_end[slot], srv->main);
-        }
         if (rc) {
             // the round could not be issued: fail its shots once the device is idle
             cudaStreamSynchronize(srv->main);

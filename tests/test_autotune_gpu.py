@@ -1,6 +1,8 @@
-"""z-chunk autotuner: the chunk length changes the launch shape, not the
-arithmetic, so every choice gives bit-identical results; the tuner records
-the fastest choice for the grid."""
+"""Work split of the fused kernels and its autotuner.  Each CTA takes bz
+consecutive planes of the grid's tile-major (tile, z) planes, in one or more
+column segments; bz changes the launch shape, not the arithmetic, so every
+choice gives bit-identical results.  The tuner records the fastest choice
+for the grid."""
 import numpy as np
 import pytest
 
@@ -29,7 +31,7 @@ def test_chunk_length_does_not_change_results_and_tuner_records_a_choice():
     kinds = ("forward", "adjoint", "imaging")
     try:
         outs = []
-        for bz in (8, 14, NZ):
+        for bz in (8, 14, NZ, 100):  # 14 and 100: CTAs whose planes span two or more columns
             for k in kinds:
                 P.tune_set(NX, NY, NZ, k, bz)
                 assert P.tune_get(NX, NY, NZ, k) == bz
