@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--dx", type=float, default=10.0)
     ap.add_argument("--model", choices=["smooth", "layered"], default="smooth",
                     help="smooth Gaussian-random TTI (full RTM workload) or layered VTI")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the modelled work split instead of timing the candidates first")
     ap.add_argument("--serve", action="store_true",
                     help="served batch: Poisson stream of RTM shots through the shot server, "
                          "against the same stream run one shot at a time in plain FP32")
@@ -266,6 +268,9 @@ def run_ours(args):
     observed = torch.empty((args.nt, nrec), dtype=torch.float32, device=dev)
     sim.forward(observed)
     sim.set_model(**model)
+    tuned = None
+    if not args.per_kernel and not args.no_autotune:
+        tuned = sim.autotune(reps=2)  # outside the timed region; picks the work split per kernel
     gvp = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev)
     grho = torch.empty_like(gvp)
     synth = torch.empty_like(observed)
@@ -373,7 +378,9 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, see config)",
         "config": {**desc, "parallelism": f"shot-parallel x{ws}" if ws > 1 else "single GPU",
                    "path": "reference kernel sequence" if args.per_kernel else "fused step kernels",
-                   "snapshots": args.snap_precision},
+                   "snapshots": args.snap_precision,
+                   "work_split": ({k: v["bz"] for k, v in tuned.items() if isinstance(v, dict)}
+                                  if tuned else "modelled")},
         "roofline": roofline, "hbm_frac_alg_per_step": hbm_frac,
         "shots_per_hour": 3600.0 * 1e3 / ms_per_step * ws,
         "passes_ms_per_shot": passes, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,

@@ -1451,6 +1451,7 @@ std::vector<int> plane_candidates(const Layout& L)
         const int bz = (nz + nch - 1) / nch;
         if (bz < 8 && nch > 1) break;
         c.push_back(bz);
+        if (nz % nch == 0) c.push_back(nz / nch);
     }
     const long long W = work_planes(L);
     const int sms = device_sms();
@@ -1483,11 +1484,21 @@ double plane_cost(const Layout& L, int bz)
     return waves * (bz + 2.0 * LAG * segs);
 }
 
-int pick_bz(const Layout& L)
+// Column-aligned shares (bz divides nz): every CTA works down whole chunks
+// of one column, and all CTAs stay at about the same z, so the halo planes
+// that neighbouring tiles share are still in L2 when the neighbour reads
+// them.  Unaligned shares balance the SMs better but spread the CTAs over
+// all of z; a kernel that stages many halo'd arrays then re-reads its halos
+// from HBM (the adjoint stages nine, the imaging kernel eleven; the forward
+// kernel three).
+bool column_aligned(const Layout& L, int bz) { return bz <= L.nz() && L.nz() % bz == 0; }
+
+int pick_bz(const Layout& L, int kind)
 {
     int best = L.nz();
     double best_cost = 1e300;
     for (int bz : plane_candidates(L)) {
+        if (kind != KIND_FWD && !column_aligned(L, bz)) continue;
         const double cost = plane_cost(L, bz);
         if (cost < best_cost - 1e-9) {
             best_cost = cost;
@@ -1709,12 +1720,12 @@ int tuned_bz(const Layout& L, int kind)
     return it == g_tuned.end() ? 0 : it->second;
 }
 
-int model_bz(const Layout& L) { return pick_bz(L); }
+int model_bz(const Layout& L, int kind) { return pick_bz(L, kind); }
 
 int choose_bz(const Layout& L, int kind)
 {
     const int t = tuned_bz(L, kind);
-    return t > 0 ? t : pick_bz(L);
+    return t > 0 ? t : pick_bz(L, kind);
 }
 
 std::vector<int> bz_candidates(const Layout& L) { return plane_candidates(L); }

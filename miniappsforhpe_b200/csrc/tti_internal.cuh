@@ -118,7 +118,7 @@ enum { KIND_FWD = 0, KIND_ADJ = 1, KIND_IMG = 2 };
 int choose_bz(const Layout& L, int kind);
 void record_tuned_bz(const Layout& L, int kind, int bz);
 int tuned_bz(const Layout& L, int kind);  // 0 if none recorded
-int model_bz(const Layout& L);            // the wave-count model's choice
+int model_bz(const Layout& L, int kind);  // the wave-count model's choice
 // Candidates the tuner tries: whole-column chunks ceil(nz/n) and equal
 // shares of the work for 1..8 CTAs per SM, each at least 8 planes.
 std::vector<int> bz_candidates(const Layout& L);

@@ -1362,7 +1362,7 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
             float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
             ms /= reps;
-            if (bz == model_bz(L)) out->model_ms[kind] = ms;
+            if (bz == model_bz(L, kind)) out->model_ms[kind] = ms;
             if (ms < best) {
                 best = ms;
                 best_bz = bz;
