@@ -61,6 +61,8 @@ def parse():
                     help="smooth Gaussian-random TTI (full RTM workload) or layered VTI")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the modelled work split instead of timing the candidates first")
+    ap.add_argument("--bz", type=int, nargs=3, default=None, metavar=("FWD", "ADJ", "IMG"),
+                    help="fixed planes per CTA of the forward, adjoint and imaging kernels (implies --no-autotune)")
     ap.add_argument("--serve", action="store_true",
                     help="served batch: Poisson stream of RTM shots through the shot server, "
                          "against the same stream run one shot at a time in plain FP32")
@@ -269,7 +271,11 @@ def run_ours(args):
     sim.forward(observed)
     sim.set_model(**model)
     tuned = None
-    if not args.per_kernel and not args.no_autotune:
+    if args.bz:
+        for kind, b in zip(("forward", "adjoint", "imaging"), args.bz):
+            P.tune_set(nx, ny, nz, kind, b)
+        tuned = {k: {"bz": b} for k, b in zip(("forward", "adjoint", "imaging"), args.bz)}
+    elif not args.per_kernel and not args.no_autotune:
         tuned = sim.autotune(reps=2)  # outside the timed region; picks the work split per kernel
     gvp = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev)
     grho = torch.empty_like(gvp)
