@@ -318,6 +318,12 @@ tti_stream_t tti_sim_stream(tti_sim* sim);
 typedef struct tti_snap_store tti_snap_store;
 
 int tti_snap_create(int nvol, const int64_t* nelem, int capacity, tti_snap_store** out);
+/* Store with a host tier: device_capacity slots in HBM, then host_capacity
+ * slots in pinned host memory (the reference's host-RAM buffers,
+ * snap_helpers/file_snap_orig.cpp:221-352); the same call sequence moves
+ * snapshots to and from either tier on the store's copy stream. */
+int tti_snap_create_tiered(int nvol, const int64_t* nelem, int device_capacity, int host_capacity,
+                           tti_snap_store** out);
 int tti_snap_destroy(tti_snap_store* s);
 /* Waits for the previous write to have drained (rtm_snap lock_for_write). */
 int tti_snap_lock_for_write(tti_snap_store* s);

@@ -98,6 +98,7 @@ _SIGS = {
     "tti_sim_read_volume": [V, I, V],
     "tti_sim_layout": [V, C.POINTER(I), C.POINTER(I), C.POINTER(I)],
     "tti_snap_create": [I, V, I, C.POINTER(V)],
+    "tti_snap_create_tiered": [I, V, I, I, C.POINTER(V)],
     "tti_snap_destroy": [V],
     "tti_snap_lock_for_write": [V],
     "tti_snap_start_write": [V, V, V],
@@ -462,13 +463,15 @@ def tune_get(nx: int, ny: int, nz: int, kind: str) -> int:
 
 
 class SnapshotStore:
-    """Device-resident LIFO snapshot store with the rtm_snap call sequence."""
+    """LIFO snapshot store with the rtm_snap call sequence: ``capacity``
+    slots in HBM, then ``host_capacity`` slots in pinned host memory."""
 
-    def __init__(self, nelems, capacity):
+    def __init__(self, nelems, capacity, host_capacity=0):
         arr = (C.c_int64 * len(nelems))(*nelems)
         self.nvol = len(nelems)
         self._h = V()
-        rc = lib().tti_snap_create(len(nelems), C.cast(arr, V), capacity, C.byref(self._h))
+        rc = lib().tti_snap_create_tiered(len(nelems), C.cast(arr, V), capacity, host_capacity,
+                                          C.byref(self._h))
         if rc != OK:
             raise TTIError(rc, "tti_snap_create")
 
