@@ -187,6 +187,44 @@ int tti_launch_init_cijs(const float* vp, const float* eps, const float* delta, 
 int tti_launch_compute_pressure(float* pressure, const float* field1, const float* field2, int64_t n,
                                 tti_stream_t stream);
 
+/* Type1 discretisation (constant density, centred second derivatives, no
+ * first-derivative stage; kernels/kernel_type1_gpu_*.cu).  Same arguments
+ * and meaning as the reference launchers; order 8 only; `simple` selects the
+ * reference's unoptimised kernels there and is accepted and ignored here (one
+ * implementation, following the optimised kernels: the reference's simple
+ * forward kernel reads the yz diagonal for the |i| >= 2 zx taps,
+ * kernels/helper_kernels_gpu.h:180-181, so the two reference kernels differ).
+ * ABx/ABy/ABz are float2 (A,B) sponge arrays; ldimz is needed to check the
+ * z halo. */
+
+/* Replaces fwd_main_loop_2_1_inner_gpu::launch (kernels/kernel_type1_gpu_fwd.h:6-9).
+ * calc_snap = 0: field3/4 += dt*rhs (use_sponge = 0) or A*f + B*dt*rhs;
+ * calc_snap = 1: rhs itself into halo-free field3/4 with ldimx_out/ldimy_out. */
+int tti_launch_type1_fwd(float* field3, float* field4, const float* field1, const float* field2, const float* model1,
+                         const float* model2, const float* model3, const float* model4, const float* model5,
+                         const float* model6, const float* model7, const float* ABx, const float* ABy,
+                         const float* ABz, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+                         int ldimx_in, int ldimy_in, int ldimz_in, int ldimx_out, int ldimy_out, int ldimz_out,
+                         float dt, double dx, double dy, double dz, int order, tti_stream_t stream, int calc_snap,
+                         int use_sponge, int simple);
+
+/* Replaces adj_main_loop_2_inner_gpu::launch (kernels/kernel_type1_gpu_adj.h:6-9):
+ * field3/4 += dt * D(M^T (field1, field2)) (or the sponge form).  Uses the
+ * library's four-float scratch over the halo'd range. */
+int tti_launch_type1_adj(float* field3, float* field4, const float* field1, const float* field2, const float* model1,
+                         const float* model2, const float* model3, const float* model4, const float* model5,
+                         const float* model6, const float* model7, const float* ABx, const float* ABy,
+                         const float* ABz, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+                         int ldimx, int ldimy, int ldimz, float dt, double dx, double dy, double dz, int order,
+                         tti_stream_t stream, int use_sponge, int simple);
+
+/* Replaces launch_update_grad_loop_kernel (kernels/kernel_type1_gpu_grad.h:4-7):
+ * grad += adj_x*snap_x + adj_z*snap_z; snapshots and gradient halo-free with
+ * leading dimensions snap_ldimx/snap_ldimy, adjoint volumes halo'd. */
+int tti_launch_type1_update_grad(const float* snap_x, const float* snap_z, float* grad_Vp, const float* adj_x,
+                                 const float* adj_z, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+                                 int snap_ldimx, int snap_ldimy, int ldimx, int ldimy, tti_stream_t stream);
+
 /* ------------------------------------------------------------------------
  * 2. Simulator object (simulator2SetUp call surface,
  *    simulator2/simulator2SetUp.h:25-35, execute at simulator2SetUp.cu:517-814).

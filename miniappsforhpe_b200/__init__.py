@@ -78,6 +78,9 @@ _SIGS = {
     "tti_launch_kernel_loop4": [V, V, I, I, I, V],
     "tti_launch_init_cijs": [V] * 13 + [L64, V],
     "tti_launch_compute_pressure": [V, V, V, L64, V],
+    "tti_launch_type1_fwd": [V] * 14 + [I] * 12 + [F, D, D, D, I, V, I, I, I],
+    "tti_launch_type1_adj": [V] * 14 + [I] * 9 + [F, D, D, D, I, V, I, I],
+    "tti_launch_type1_update_grad": [V] * 5 + [I] * 10 + [V],
     "tti_sim_create": [C.POINTER(SimConfig), C.POINTER(V)],
     "tti_sim_footprint_bytes": [C.POINTER(SimConfig), C.POINTER(L64)],
     "tti_sim_destroy": [V],
@@ -190,6 +193,33 @@ def launch_adj_kernel2_drv(dfield1dx, dfield2dx, dfield1dy, dfield2dy, dfield1dz
           dfield2dz, field3_rhs, field4_rhs, field1, field2, Model11, model1, model2, model3, model4,
           model5, model6, model7, ixbeg, ixend, iybeg, iyend, izbeg, izend, invdxx, invdyy, invdzz,
           invdxy, invdyz, invdzx, ldimx, ldimy, order, dt, invdx, invdy, invdz, stream)
+
+
+def launch_type1_fwd(field3, field4, field1, field2, model1, model2, model3, model4, model5, model6,
+                     model7, ABx, ABy, ABz, ixbeg, ixend, iybeg, iyend, izbeg, izend, ldimx_in, ldimy_in,
+                     ldimz_in, ldimx_out, ldimy_out, ldimz_out, dt, dx, dy, dz, order=8, stream=None,
+                     calc_snap=False, use_sponge=False, simple=False):
+    """kernels/kernel_type1_gpu_fwd.h:6-9 (fwd_main_loop_2_1_inner_gpu::launch)."""
+    _call("tti_launch_type1_fwd", field3, field4, field1, field2, model1, model2, model3, model4, model5,
+          model6, model7, ABx, ABy, ABz, ixbeg, ixend, iybeg, iyend, izbeg, izend, ldimx_in, ldimy_in,
+          ldimz_in, ldimx_out, ldimy_out, ldimz_out, dt, dx, dy, dz, order, stream, int(calc_snap),
+          int(use_sponge), int(simple))
+
+
+def launch_type1_adj(field3, field4, field1, field2, model1, model2, model3, model4, model5, model6,
+                     model7, ABx, ABy, ABz, ixbeg, ixend, iybeg, iyend, izbeg, izend, ldimx, ldimy, ldimz, dt,
+                     dx, dy, dz, order=8, stream=None, use_sponge=False, simple=False):
+    """kernels/kernel_type1_gpu_adj.h:6-9 (adj_main_loop_2_inner_gpu::launch)."""
+    _call("tti_launch_type1_adj", field3, field4, field1, field2, model1, model2, model3, model4, model5,
+          model6, model7, ABx, ABy, ABz, ixbeg, ixend, iybeg, iyend, izbeg, izend, ldimx, ldimy, ldimz, dt, dx,
+          dy, dz, order, stream, int(use_sponge), int(simple))
+
+
+def launch_type1_update_grad(snap_x, snap_z, grad_Vp, adj_x, adj_z, ixbeg, ixend, iybeg, iyend, izbeg, izend,
+                             snap_ldimx, snap_ldimy, ldimx, ldimy, stream=None):
+    """kernels/kernel_type1_gpu_grad.h:4-7 (launch_update_grad_loop_kernel)."""
+    _call("tti_launch_type1_update_grad", snap_x, snap_z, grad_Vp, adj_x, adj_z, ixbeg, ixend, iybeg, iyend,
+          izbeg, izend, snap_ldimx, snap_ldimy, ldimx, ldimy, stream)
 
 
 def launch_update_adj_kernel_main_3(field3, field4, field1_dx, field2_dx, field1_dy, field2_dy,

@@ -533,6 +533,9 @@ inline cudaStream_t S(tti_stream_t s) { return reinterpret_cast<cudaStream_t>(s)
 
 } // namespace
 
+// The library's per-device scratch of four floats per cell (grown on demand).
+float4* library_scratch(size_t nelem) { return scratch_base(nelem); }
+
 // Launch helpers used by the simulator (same kernels as the C ABI).
 int launch_base(const float* f1, const float* f2, const float* m1, const float* m2, const float* m3,
                 const float* m4, float4* base, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,

@@ -110,6 +110,9 @@ _SIGS = {
     "orc_pressure": [V, V, V, L],
     "orc_fwd_step": [C.POINTER(OrcGrid)] + [V] * 21 + [L, F, I, V, V],
     "orc_adj_step": [C.POINTER(OrcGrid)] + [V] * 23 + [I, V, V],
+    "orc_t1_fwd": [V] * 14 + [I] * 10 + [F, D, D, D, I],
+    "orc_t1_adj": [V] * 14 + [I] * 8 + [F, D, D, D, I],
+    "orc_t1_grad": [V] * 5 + [I] * 10,
     "orc_num_threads": [],
 }
 
@@ -213,6 +216,23 @@ class Oracle:
                                     _p(m["irho"]), _p(m["m1"]), _p(m["m2"]), _p(m["m3"]),
                                     _p(m["m4"]), _p(m["rx"]), _p(m["ry"]), _p(m["rz"]), *lay.ranges,
                                     lay.ldimx, lay.ldimy, gx, gy, *h)
+
+    # Type1 (constant density, centred): tests/test_type1*.py.
+    def t1_fwd(self, lay: Layout, f3, f4, f1, f2, m, ab, dt, h, mode, out_ld=None):
+        """mode 0: f3,f4 += dt*rhs; 1: sponge form; 2: rhs into halo-free f3,f4 (out_ld = (ldx, ldy))."""
+        ox, oy = out_ld if out_ld else (lay.ldimx, lay.ldimy)
+        self.fn["orc_t1_fwd"](_p(f3), _p(f4), _p(f1), _p(f2), _p(m["m1"]), _p(m["m2"]), _p(m["m3"]),
+                              _p(m["m4"]), _p(m["rx"]), _p(m["ry"]), _p(m["rz"]), _p(ab[0]), _p(ab[1]),
+                              _p(ab[2]), *lay.ranges, lay.ldimx, lay.ldimy, ox, oy, dt, *h, mode)
+
+    def t1_adj(self, lay: Layout, f3, f4, f1, f2, m, ab, dt, h, sponge):
+        self.fn["orc_t1_adj"](_p(f3), _p(f4), _p(f1), _p(f2), _p(m["m1"]), _p(m["m2"]), _p(m["m3"]),
+                              _p(m["m4"]), _p(m["rx"]), _p(m["ry"]), _p(m["rz"]), _p(ab[0]), _p(ab[1]),
+                              _p(ab[2]), *lay.ranges, lay.ldimx, lay.ldimy, dt, *h, int(sponge))
+
+    def t1_grad(self, lay: Layout, snap_x, snap_z, grad, adj_x, adj_z):
+        self.fn["orc_t1_grad"](_p(snap_x), _p(snap_z), _p(grad), _p(adj_x), _p(adj_z), *lay.ranges,
+                               lay.nx, lay.ny, lay.ldimx, lay.ldimy)
 
     def init_cijs(self, vp, eps, delta, vs, theta, phi):
         n = vp.size

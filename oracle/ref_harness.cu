@@ -16,6 +16,9 @@
 #include <cuda_runtime.h>
 #include <cstdio>
 
+#include "kernel_type1_gpu_adj.h"
+#include "kernel_type1_gpu_fwd.h"
+#include "kernel_type1_gpu_grad.h"
 #include "kernel_type2_adj.h"
 #include "kernel_type2_fwd.h"
 #include "kernel_type2_fwd_drv.h"
@@ -161,6 +164,47 @@ int ref_loop4(float* f1, float* f2, int ldimx, int ldimy, int izbeg)
     dim3 threads(1024, 1, 1);
     dim3 blocks((stride - 1) / 1024 + 1, 1, izbeg + 1);
     kernel_loop4_kernel<<<blocks, threads>>>(f1, f2, stride, izbeg);
+    return status();
+}
+
+// Type1 launchers (kernels/kernel_type1_gpu_{fwd,adj,grad}.cu), default
+// (optimised) kernels, standard layout only (ldimz = izend + 5).
+int ref_t1_fwd(float* f3, float* f4, const float* f1, const float* f2, const float* m1, const float* m2,
+               const float* m3, const float* m4, const float* m5, const float* m6, const float* m7, const float* abx,
+               const float* aby, const float* abz, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+               int ldimx, int ldimy, int ldimz, int ldimx_out, int ldimy_out, int ldimz_out, float dt, double dx,
+               double dy, double dz, int calc_snap, int use_sponge)
+{
+    if (!layout_ok(ixbeg, ixend, iybeg, iyend, izbeg, izend, ldimx, ldimy) || ldimz != izend + 5) return 2;
+    if (calc_snap && use_sponge) return 2;
+    if (!calc_snap && (ldimx_out != ldimx || ldimy_out != ldimy)) return 2;
+    fwd_main_loop_2_1_inner_gpu::launch(f3, f4, f1, f2, m1, m2, m3, m4, m5, m6, m7,
+                                        reinterpret_cast<const float2*>(abx), reinterpret_cast<const float2*>(aby),
+                                        reinterpret_cast<const float2*>(abz), ixbeg, ixend, iybeg, iyend, izbeg,
+                                        izend, ldimx, ldimy, ldimz, ldimx_out, ldimy_out, ldimz_out, dt, dx, dy, dz, 8,
+                                        0, calc_snap != 0, use_sponge != 0, false);
+    return status();
+}
+
+int ref_t1_adj(float* f3, float* f4, const float* f1, const float* f2, const float* m1, const float* m2,
+               const float* m3, const float* m4, const float* m5, const float* m6, const float* m7, const float* abx,
+               const float* aby, const float* abz, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,
+               int ldimx, int ldimy, int ldimz, float dt, double dx, double dy, double dz, int use_sponge)
+{
+    if (!layout_ok(ixbeg, ixend, iybeg, iyend, izbeg, izend, ldimx, ldimy) || ldimz != izend + 5) return 2;
+    adj_main_loop_2_inner_gpu::launch(f3, f4, f1, f2, m1, m2, m3, m4, m5, m6, m7,
+                                      reinterpret_cast<const float2*>(abx), reinterpret_cast<const float2*>(aby),
+                                      reinterpret_cast<const float2*>(abz), ixbeg, ixend, iybeg, iyend, izbeg, izend,
+                                      ldimx, ldimy, ldimz, dt, dx, dy, dz, 8, 0, use_sponge != 0, false);
+    return status();
+}
+
+int ref_t1_grad(float* snap_x, float* snap_z, float* grad, float* adj_x, float* adj_z, int ixbeg, int ixend,
+                int iybeg, int iyend, int izbeg, int izend, int snx, int sny, int ldimx, int ldimy)
+{
+    if (!layout_ok(ixbeg, ixend, iybeg, iyend, izbeg, izend, ldimx, ldimy)) return 2;
+    launch_update_grad_loop_kernel(volume_index(snx, sny), volume_index(ldimx, ldimy), snap_x, snap_z, grad, adj_x,
+                                   adj_z, ixbeg, ixend, iybeg, iyend, izbeg, izend);
     return status();
 }
 

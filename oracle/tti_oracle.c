@@ -649,6 +649,225 @@ void FN(orc_adj_step)(const orc_grid* g, real* f1, real* f2, real* f3, real* f4,
     if (g->free_surface) FN(orc_loop4)(f1, f2, ldimx, ldimy, g->izbeg);
 }
 
+/* ------------------------------------------------------------------------
+ * Type1 discretisation (kernels/kernel_type1_gpu_{fwd,adj,grad}.cu): the
+ * constant-density TTI operator with centred second derivatives (DF2
+ * coefficients on the normal directions, the same diagonal form for the
+ * mixed ones) and no separate first-derivative stage.  The restatement
+ * follows the launchers' default (optimised) kernels:
+ * fwd_main_loop_2_1 (kernel_type1_gpu_fwd.cu:150-232 for the derivative
+ * sums, :122-146 for V/H and the right-hand sides) and adj_main_loop_2
+ * (kernel_type1_gpu_adj.cu:103-235).  Finite-difference constants as
+ * kernel_utils::compute_fd_const: invdxx = 1/dx^2, invdxy = 1/(4 dx dy), ...
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    real xx, yy, zz, xy, yz, zx;
+} t1_drv;
+
+/* Centred second derivatives of f at i (strides sx = 1, sy = ldimx, sz). */
+static inline t1_drv t1_derivs(const real* f, i64 i, i64 sy, i64 sz, real ixx, real iyy, real izz,
+                               real ixy, real iyz, real izx)
+{
+    t1_drv d;
+    /* z terms in plane order iz-4 .. iz+4 (compute_z_contributions, :150-185) */
+    real zz = 0, zx = 0, yz = 0;
+    for (int ir = -4; ir <= 4; ++ir) {
+        real c = (real)C2[ir < 0 ? -ir : ir];
+        i64 j = i + ir * sz;
+        zz = zz + c * f[j];
+        if (ir != 0) {
+            zx = zx + c * (f[j + ir] - f[j - ir]);
+            yz = yz + c * (f[j + ir * sy] - f[j - ir * sy]);
+        }
+    }
+    d.zz = zz * izz;
+    d.zx = zx * izx;
+    d.yz = yz * iyz;
+    /* x and y terms (compute_xy_contributions, :190-232) */
+    real xx = (real)C2[0] * f[i], yy = (real)C2[0] * f[i], xy = 0;
+    for (int k = 1; k <= 4; ++k) {
+        real c = (real)C2[k];
+        xx += c * (f[i + k] + f[i - k]);
+        yy += c * (f[i + k * sy] + f[i - k * sy]);
+        xy += c * (f[i + k * sy + k] - f[i + k * sy - k] + f[i - k * sy - k] - f[i - k * sy + k]);
+    }
+    d.xx = xx * ixx;
+    d.yy = yy * iyy;
+    d.xy = xy * ixy;
+    return d;
+}
+
+/* mode 0: f3 += dt*rhs, f4 += dt*rhs (no sponge);  mode 1: f = A f + B rhs dt
+ * (sponge, A,B = min over the axis profiles);  mode 2 (calc_snap): the
+ * right-hand sides themselves into halo-free outputs with ldimx_out/ldimy_out.
+ * In modes 0 and 1 outputs use the input strides (the reference offsets the
+ * output base with the input dimensions, kernel_type1_gpu_fwd.cu:488-492). */
+void FN(orc_t1_fwd)(real* f3, real* f4, const real* f1, const real* f2, const real* m1, const real* m2,
+                    const real* m3, const real* m4, const real* m5, const real* m6, const real* m7,
+                    const float* abx, const float* aby, const float* abz, int ixbeg, int ixend, int iybeg,
+                    int iyend, int izbeg, int izend, int ldimx, int ldimy, int ldimx_out, int ldimy_out,
+                    float dt, double dx, double dy, double dz, int mode)
+{
+    const real ixx = (real)(float)(1.0 / (dx * dx)), iyy = (real)(float)(1.0 / (dy * dy)),
+               izz = (real)(float)(1.0 / (dz * dz));
+    const real ixy = (real)(float)(1.0 / (4 * dx * dy)), iyz = (real)(float)(1.0 / (4 * dy * dz)),
+               izx = (real)(float)(1.0 / (4 * dx * dz));
+    const i64 sy = ldimx, sz = (i64)ldimx * ldimy;
+#pragma omp parallel for schedule(static)
+    for (int iz = izbeg; iz <= izend; ++iz)
+        for (int iy = iybeg; iy <= iyend; ++iy)
+            for (int ix = ixbeg; ix <= ixend; ++ix) {
+                i64 i = IDX(ix, iy, iz);
+                t1_drv a = t1_derivs(f1, i, sy, sz, ixx, iyy, izz, ixy, iyz, izx);
+                t1_drv b = t1_derivs(f2, i, sy, sz, ixx, iyy, izz, ixy, iyz, izx);
+                real rx = m5[i], ry = m6[i], rz = m7[i];
+                real rxx = rx * rx, ryy = ry * ry, rzz = rz * rz;
+                real rxy = (real)2 * rx * ry, ryz = (real)2 * ry * rz, rzx = (real)2 * rz * rx;
+                real V1 = rxx * a.xx + ryy * a.yy + rzz * a.zz + rxy * a.xy + rzx * a.zx + ryz * a.yz;
+                real H1 = a.xx + a.yy + a.zz - V1;
+                real V2 = rxx * b.xx + ryy * b.yy + rzz * b.zz + rxy * b.xy + rzx * b.zx + ryz * b.yz;
+                real H2 = b.xx + b.yy + b.zz - V2;
+                real r3 = m1[i] * H1 + m4[i] * V1 + m2[i] * V2;
+                real r4 = m2[i] * H1 + m3[i] * V2 + m4[i] * H2;
+                if (mode == 2) {
+                    i64 o = ((i64)(iz - izbeg) * ldimy_out + (iy - iybeg)) * ldimx_out + (ix - ixbeg);
+                    f3[o] = r3;
+                    f4[o] = r4;
+                } else if (mode == 1) {
+                    real A = fminf(abx[2 * ix], fminf(aby[2 * iy], abz[2 * iz]));
+                    real B = fminf(abx[2 * ix + 1], fminf(aby[2 * iy + 1], abz[2 * iz + 1]));
+                    f3[i] = A * f3[i] + B * r3 * (real)dt;
+                    f4[i] = A * f4[i] + B * r4 * (real)dt;
+                } else {
+                    f3[i] += r3 * (real)dt;
+                    f4[i] += r4 * (real)dt;
+                }
+            }
+}
+
+/* Adjoint temporaries at j (compute_temp_arrays, kernel_type1_gpu_adj.cu:103-153):
+ * lap/hz of both fields, weighted per derivative by r_a r_b. */
+typedef struct {
+    real lx, hx, lz, hz;
+} t1_base;
+static inline t1_base t1_base_at(const real* f1, const real* f2, const real* m1, const real* m2,
+                                 const real* m3, const real* m4, i64 j)
+{
+    t1_base b;
+    b.lx = m1[j] * f1[j] + m2[j] * f2[j];
+    b.hx = (-m1[j] + m4[j]) * f1[j] - m2[j] * f2[j];
+    b.lz = m4[j] * f2[j];
+    b.hz = m2[j] * f1[j] + (-m4[j] + m3[j]) * f2[j];
+    return b;
+}
+
+void FN(orc_t1_adj)(real* f3, real* f4, const real* f1, const real* f2, const real* m1, const real* m2,
+                    const real* m3, const real* m4, const real* m5, const real* m6, const real* m7,
+                    const float* abx, const float* aby, const float* abz, int ixbeg, int ixend, int iybeg,
+                    int iyend, int izbeg, int izend, int ldimx, int ldimy, float dt, double dx, double dy,
+                    double dz, int use_sponge)
+{
+    const real ixx = (real)(float)(1.0 / (dx * dx)), iyy = (real)(float)(1.0 / (dy * dy)),
+               izz = (real)(float)(1.0 / (dz * dz));
+    const real ixy = (real)(float)(1.0 / (4 * dx * dy)), iyz = (real)(float)(1.0 / (4 * dy * dz)),
+               izx = (real)(float)(1.0 / (4 * dx * dz));
+    const i64 sy = ldimx, sz = (i64)ldimx * ldimy;
+#define T1_W(j, w1, w2, lap, o3, o4)                                                                 \
+    do {                                                                                             \
+        t1_base b_ = t1_base_at(f1, f2, m1, m2, m3, m4, (j));                                        \
+        real w_ = (w1) * (w2);                                                                       \
+        o3 = ((lap) ? b_.lx : (real)0) + w_ * b_.hx;                                                 \
+        o4 = ((lap) ? b_.lz : (real)0) + w_ * b_.hz;                                                 \
+    } while (0)
+#pragma omp parallel for schedule(static)
+    for (int iz = izbeg; iz <= izend; ++iz)
+        for (int iy = iybeg; iy <= iyend; ++iy)
+            for (int ix = ixbeg; ix <= ixend; ++ix) {
+                i64 i = IDX(ix, iy, iz);
+                real s3 = 0, s4 = 0, t3, t4, u3, u4;
+                /* z terms, planes iz-4 .. iz+4 (compute_z_contributions, :162-186) */
+                for (int ir = -4; ir <= 4; ++ir) {
+                    real c = (real)C2[ir < 0 ? -ir : ir];
+                    i64 j = i + ir * sz;
+                    T1_W(j, m7[j], m7[j], 1, t3, t4);
+                    real a3 = izz * c * t3, a4 = izz * c * t4;
+                    if (ir != 0) {
+                        i64 jp = j + ir * sy, jm = j - ir * sy;
+                        T1_W(jp, (real)2 * m6[jp], m7[jp], 0, t3, t4);
+                        T1_W(jm, (real)2 * m6[jm], m7[jm], 0, u3, u4);
+                        a3 = a3 + iyz * c * (t3 - u3);
+                        a4 = a4 + iyz * c * (t4 - u4);
+                        jp = j + ir;
+                        jm = j - ir;
+                        T1_W(jp, (real)2 * m7[jp], m5[jp], 0, t3, t4);
+                        T1_W(jm, (real)2 * m7[jm], m5[jm], 0, u3, u4);
+                        a3 = a3 + izx * c * (t3 - u3);
+                        a4 = a4 + izx * c * (t4 - u4);
+                    }
+                    s3 = s3 + a3;
+                    s4 = s4 + a4;
+                }
+                /* x and y terms (compute_xy_contributions, :191-217) */
+                real xx3, xx4, yy3, yy4, xy3 = 0, xy4 = 0;
+                T1_W(i, m5[i], m5[i], 1, t3, t4);
+                xx3 = (real)C2[0] * t3;
+                xx4 = (real)C2[0] * t4;
+                T1_W(i, m6[i], m6[i], 1, t3, t4);
+                yy3 = (real)C2[0] * t3;
+                yy4 = (real)C2[0] * t4;
+                for (int k = 1; k <= 4; ++k) {
+                    real c = (real)C2[k];
+                    i64 jp = i + k, jm = i - k;
+                    T1_W(jp, m5[jp], m5[jp], 1, t3, t4);
+                    T1_W(jm, m5[jm], m5[jm], 1, u3, u4);
+                    xx3 += c * (t3 + u3);
+                    xx4 += c * (t4 + u4);
+                    jp = i + k * sy;
+                    jm = i - k * sy;
+                    T1_W(jp, m6[jp], m6[jp], 1, t3, t4);
+                    T1_W(jm, m6[jm], m6[jm], 1, u3, u4);
+                    yy3 += c * (t3 + u3);
+                    yy4 += c * (t4 + u4);
+                    real p3, p4, q3, q4, r3, r4, w3, w4;
+                    i64 jpp = i + k * sy + k, jpm = i + k * sy - k, jmm = i - k * sy - k, jmp = i - k * sy + k;
+                    T1_W(jpp, (real)2 * m5[jpp], m6[jpp], 0, p3, p4);
+                    T1_W(jpm, (real)2 * m5[jpm], m6[jpm], 0, q3, q4);
+                    T1_W(jmm, (real)2 * m5[jmm], m6[jmm], 0, r3, r4);
+                    T1_W(jmp, (real)2 * m5[jmp], m6[jmp], 0, w3, w4);
+                    xy3 += c * (p3 - q3 + r3 - w3);
+                    xy4 += c * (p4 - q4 + r4 - w4);
+                }
+                s3 += ixx * xx3 + iyy * yy3 + ixy * xy3;
+                s4 += ixx * xx4 + iyy * yy4 + ixy * xy4;
+                if (use_sponge) {
+                    real A = fminf(abx[2 * ix], fminf(aby[2 * iy], abz[2 * iz]));
+                    real B = fminf(abx[2 * ix + 1], fminf(aby[2 * iy + 1], abz[2 * iz + 1]));
+                    f3[i] = A * f3[i] + B * s3 * (real)dt;
+                    f4[i] = A * f4[i] + B * s4 * (real)dt;
+                } else {
+                    f3[i] += s3 * (real)dt;
+                    f4[i] += s4 * (real)dt;
+                }
+            }
+#undef T1_W
+}
+
+/* Type1 imaging: grad += adj_x*snap_x + adj_z*snap_z over the interior
+ * (kernel_type1_gpu_grad.cu:4-21); snapshots and gradient are halo-free. */
+void FN(orc_t1_grad)(const real* snap_x, const real* snap_z, real* grad, const real* adj_x, const real* adj_z,
+                     int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend, int sldx, int sldy,
+                     int ldimx, int ldimy)
+{
+#pragma omp parallel for schedule(static)
+    for (int iz = izbeg; iz <= izend; ++iz)
+        for (int iy = iybeg; iy <= iyend; ++iy)
+            for (int ix = ixbeg; ix <= ixend; ++ix) {
+                i64 d = ((i64)(iz - izbeg) * sldy + (iy - iybeg)) * sldx + (ix - ixbeg);
+                i64 i = IDX(ix, iy, iz);
+                grad[d] += adj_x[i] * snap_x[d] + adj_z[i] * snap_z[d];
+            }
+}
+
 int FN(orc_num_threads)(void)
 {
 #ifdef _OPENMP
