@@ -336,6 +336,11 @@ void scheduler_main(tti_server* srv)
         for (Shot* s : active) {
             if (s->planned_left <= 0) continue;
             int64_t u = (int64_t)std::floor(srv->cfg.round_ms / s->unit_ms);
+            // whole imaging periods, so that consecutive rounds of a shot have
+            // the same launch pattern and the captured graph can be updated in
+            // place instead of instantiated again
+            const int64_t period = std::max(1, s->req.xcorr_step);
+            if (u >= period) u -= u % period;
             u = std::max<int64_t>(1, std::min(u, s->planned_left));
             plan.push_back({s, u});
             s->planned_left -= u;
