@@ -287,6 +287,15 @@ int tti_sim_adjoint(tti_sim* sim, const float* residual, int residual_on_device)
  * traces of the last forward run minus these observed traces (nt*nrec). */
 int tti_sim_adjoint_observed(tti_sim* sim, const float* observed, int observed_on_device);
 
+/* Failure-detection self-check (no reference counterpart; the reference
+ * aborts instead).  Every wait inside the fused kernels is bounded: a wait
+ * that runs out records a timeout that the simulator returns as
+ * TTI_ETIMEOUT, and the kernel returns, leaving the context usable.  This
+ * runs that path on a shared-memory barrier that nothing completes, with a
+ * limit of `seconds` (0 < seconds <= 10) of SM clock cycles; it returns
+ * TTI_ETIMEOUT when the wait gave up and reported as it should. */
+int tti_selfcheck_bounded_wait(double seconds, tti_stream_t stream);
+
 /* z-chunk autotuner.  The fused kernels run one CTA per SM on TX x TY
  * column tiles (TX = 32, TY = 16) marching along z; the grid's planes are
  * split among CTAs in tile-major order, bz consecutive planes per CTA (one

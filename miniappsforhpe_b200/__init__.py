@@ -96,6 +96,7 @@ _SIGS = {
     "tti_sim_kernel_times": [V, V, V],
     "tti_sim_autotune": [V, I, C.POINTER(TuneReport)],
     "tti_tune_set": [I, I, I, I, I],
+    "tti_selfcheck_bounded_wait": [D, V],
     "tti_tune_get": [I, I, I, I],
     "tti_sim_volume": [V, I, C.POINTER(V)],
     "tti_sim_read_volume": [V, I, V],

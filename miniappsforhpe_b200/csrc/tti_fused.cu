@@ -1693,6 +1693,50 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
 int prepare_fused_kernels() { return kernels_prepared() ? TTI_OK : TTI_ELAUNCH; }
 
 namespace {
+// One CTA waits on a shared-memory mbarrier that expects bytes no copy will
+// deliver: the bounded wait of the fused kernels gives up after its clock
+// limit, records the timeout in the error word and the kernel returns.
+// Nothing is in flight when it does.
+__global__ void k_wait_selfcheck(int* err, unsigned long long limit)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_expect_tx(&bar, 16u);
+    __syncthreads();
+    if (mbar_try_wait(&bar, 0)) return;  // cannot complete: no copy was issued
+    const long long t0 = clock64();
+    while (!mbar_try_wait(&bar, 0))
+        if ((unsigned long long)(clock64() - t0) > limit) {
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            return;
+        }
+}
+} // namespace
+
+int wait_selfcheck(cudaStream_t st, long long limit_cycles)
+{
+    int* w = nullptr;
+    if (cudaMallocAsync(&w, sizeof(int), st) != cudaSuccess) {
+        cudaGetLastError();
+        return TTI_ENOMEM;
+    }
+    cudaMemsetAsync(w, 0, sizeof(int), st);
+    k_wait_selfcheck<<<1, 32, 0, st>>>(w, (unsigned long long)limit_cycles);
+    int rc = launch_status();
+    if (!rc) rc = fused_wait_status(st, w);
+    cudaFreeAsync(w, st);
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    return rc;
+}
+
+
+
+namespace {
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, int> g_tuned;  // (device, nx, ny, nz, kind) -> bz
 int current_device()

@@ -132,4 +132,8 @@ std::vector<int> bz_candidates(const Layout& L);
 // capture that contains fused launches.
 int prepare_fused_kernels();
 
+// Runs the bounded-wait path on a barrier that never completes; returns
+// TTI_ETIMEOUT when the wait gave up and reported as it should.
+int wait_selfcheck(cudaStream_t st, long long limit_cycles);
+
 } // namespace tti

@@ -83,6 +83,8 @@ struct tti_server {
 
 namespace {
 
+constexpr int64_t kMaxUnitsPerRound = 128;  // fused steps of one shot in one round
+
 tti_sim_config shot_config(const tti_server* srv, const tti_shot_request& r, int ckpt)
 {
     tti_sim_config c{};
@@ -340,6 +342,9 @@ void scheduler_main(tti_server* srv)
             // the same launch pattern and the captured graph can be updated in
             // place instead of instantiated again
             const int64_t period = std::max(1, s->req.xcorr_step);
+            // a small grid's round would otherwise hold thousands of launches
+            // whose capture and update cost host time the device waits for
+            u = std::min<int64_t>(u, kMaxUnitsPerRound);
             if (u >= period) u -= u % period;
             u = std::max<int64_t>(1, std::min(u, s->planned_left));
             plan.push_back({s, u});

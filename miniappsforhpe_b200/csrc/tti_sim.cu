@@ -1381,6 +1381,18 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
     return rc;
 }
 
+int tti_selfcheck_bounded_wait(double seconds, tti_stream_t stream)
+{
+    if (!(seconds > 0) || seconds > 10) return TTI_EINVAL;
+    int dev = 0, khz = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return TTI_ELAUNCH;
+    }
+    const long long cycles = (long long)(seconds * khz * 1e3);
+    return wait_selfcheck(reinterpret_cast<cudaStream_t>(stream), cycles);
+}
+
 int tti_tune_set(int nx, int ny, int nz, int kind, int bz)
 {
     if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind > 2 || bz < 0) return TTI_EINVAL;
