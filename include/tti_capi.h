@@ -251,6 +251,9 @@ typedef struct {
                              Results are identical to K = 0. */
     int use_graphs;       /* 1: each time loop (or checkpoint segment) is captured into a CUDA graph
                              and launched as one; the instantiated graph is reused across calls */
+    int scheme;           /* 0: staggered variable-density operator (kernel_type2, the simulator's
+                             own); 1: centred constant-density operator (kernel_type1 launchers;
+                             Vp image only, grad_rho stays zero) */
 } tti_sim_config;
 
 int tti_sim_create(const tti_sim_config* cfg, tti_sim** out);

@@ -262,6 +262,7 @@ int validate(const tti_sim_config& c)
         !(c.dz > 0) || !(c.dt > 0) || c.sponge_width < 0 || (c.nz <= kRadius && c.free_surface))
         return TTI_EINVAL;
     if (c.snap_precision < 0 || c.snap_precision > 2) return TTI_EINVAL;
+    if (c.scheme < 0 || c.scheme > 1) return TTI_EINVAL;
     if (c.snap_precision != 0 && (!c.fused || c.nx % 8 != 0)) return TTI_EINVAL;
     if (c.checkpoint_every < 0) return TTI_EINVAL;
     if (c.checkpoint_every > 0 && (c.checkpoint_every % c.xcorr_step != 0 || !c.fused || !c.save_snapshots))
@@ -285,7 +286,8 @@ Plan plan_of(const tti_sim_config& c)
     const size_t nin = (size_t)c.nx * c.ny * c.nz;
     pl.core = 6 * vb + 8 * vb + 2 * nin * sizeof(float) + (size_t)c.nt * sizeof(float) +
               (size_t)(L.ldimx + L.ldimy + L.ldimz) * sizeof(float2) + sizeof(int);
-    pl.need_aux = !c.fused || (c.save_snapshots && !fused_image_supported(L));
+    // derivative volumes and scratch: only the staggered scheme's kernel sequence
+    pl.need_aux = c.scheme == 0 && (!c.fused || (c.save_snapshots && !fused_image_supported(L)));
     if (pl.need_aux) pl.aux = 10 * vb + 4 * vb;  // rhs3, rhs4, snp, snq, six derivatives, 4-float scratch
     if (c.save_snapshots) {
         pl.nsnap = (c.nt - 1) / c.xcorr_step + 1;
@@ -395,6 +397,20 @@ int forward_per_kernel_step(tti_sim* s, int n, cudaStream_t st)
         if ((rc = tti_launch_kernel_loop4(w.p, w.q, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
         s->launches++;
     }
+    if (c.scheme == 1) {  // centred constant-density operator (kernels/kernel_type1_gpu_fwd.cu)
+        if ((rc = tti_launch_type1_fwd(w.pd, w.qd, w.p, w.q, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->mv[5],
+                                       s->mv[6], s->mv[7], (const float*)s->abx, (const float*)s->aby,
+                                       (const float*)s->abz, L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg, L.izend,
+                                       L.ldimx, L.ldimy, L.ldimz, L.ldimx, L.ldimy, L.ldimz, c.dt, c.dx, c.dy, c.dz,
+                                       8, st, 0, s->sponge_active ? 1 : 0, 0)))
+            return rc;
+        s->launches++;
+        if (s->src_index >= 0) {
+            k_add_source<<<1, 1, 0, st>>>(w.pd, w.qd, s->src_index, s->wavelet[n] * c.dt);
+            s->launches++;
+        }
+        return launch_status();
+    }
     if ((rc = tti_launch_fwd_kernel2_drv(w.p, w.q, s->mv[0], s->d[0], s->d[1], s->d[2], s->d[3], s->d[4], s->d[5],
                                          L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg, L.izend, (float)(1.0 / c.dx),
                                          (float)(1.0 / c.dy), (float)(1.0 / c.dz), L.ldimx, L.ldimy, 8, st)))
@@ -426,6 +442,25 @@ int adjoint_per_kernel_step(tti_sim* s, cudaStream_t st)
     const Layout& L = s->L;
     const tti_sim_config& c = s->cfg;
     WaveState& w = s->w;
+    if (c.scheme == 1) {  // kernels/kernel_type1_gpu_adj.cu, then loop2 and loop4
+        int rc = tti_launch_type1_adj(w.pd, w.qd, w.p, w.q, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->mv[5],
+                                      s->mv[6], s->mv[7], (const float*)s->abx, (const float*)s->aby,
+                                      (const float*)s->abz, L.ixbeg, L.ixend, L.iybeg, L.iyend, L.izbeg, L.izend,
+                                      L.ldimx, L.ldimy, L.ldimz, c.dt, c.dx, c.dy, c.dz, 8, st,
+                                      s->sponge_active ? 1 : 0, 0);
+        if (rc) return rc;
+        s->launches += 2;
+        if ((rc = tti_launch_kernel_loop2(w.p, w.q, w.pd, w.qd, L.ldimx, L.ldimy, L.ixbeg, L.ixend, L.iybeg,
+                                          L.iyend, L.izbeg, L.izend, (const float*)s->abx, (const float*)s->aby,
+                                          (const float*)s->abz, c.dt, st)))
+            return rc;
+        s->launches++;
+        if (c.free_surface) {
+            if ((rc = tti_launch_kernel_loop4(w.p, w.q, L.ldimx, L.ldimy, L.izbeg, st))) return rc;
+            s->launches++;
+        }
+        return TTI_OK;
+    }
     int rc = launch_base(w.p, w.q, s->mv[1], s->mv[2], s->mv[3], s->mv[4], s->base, L.ixbeg, L.ixend, L.iybeg, L.iyend,
                          L.izbeg, L.izend, L.ldimx, L.ldimy, st);
     if (rc) return rc;
@@ -470,6 +505,12 @@ int image_per_kernel(tti_sim* s, const float* slot, cudaStream_t st)
     const tti_sim_config& c = s->cfg;
     WaveState& w = s->w;
     int64_t n = s->ninterior;
+    if (c.scheme == 1) {  // kernels/kernel_type1_gpu_grad.cu: Vp image only
+        int rc = tti_launch_type1_update_grad(slot, slot + n, s->grad_vp, w.pd, w.qd, L.ixbeg, L.ixend, L.iybeg,
+                                              L.iyend, L.izbeg, L.izend, L.nx(), L.ny(), L.ldimx, L.ldimy, st);
+        s->launches++;
+        return rc;
+    }
     int rc = tti_launch_update_Vp_gradient(slot, slot + n, s->grad_vp, w.pd, w.qd, L.ixbeg, L.ixend, L.iybeg, L.iyend,
                                            L.izbeg, L.izend, L.nx(), L.ny(), L.ldimx, L.ldimy, st);
     if (rc) return rc;
@@ -557,7 +598,8 @@ int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t s
     a.dz = c.dz;
     a.err = s->err;
     mark_begin(s, 0, st);
-    int rc = launch_fused_forward(s->L, a, st);
+    int rc = c.scheme == 1 ? launch_t1_fused_forward(s->L, a, s->sponge_active ? 1 : 0, st)
+                           : launch_fused_forward(s->L, a, st);
     mark_end(s, st);
     if (rc) return rc;
     s->launches++;
@@ -589,7 +631,7 @@ int fused_adjoint_step(tti_sim* s, cudaStream_t st)
     a.dz = c.dz;
     a.err = s->err;
     mark_begin(s, 1, st);
-    int rc = launch_fused_adjoint(s->L, a, st);
+    int rc = c.scheme == 1 ? launch_t1_fused_adjoint(s->L, a, st) : launch_fused_adjoint(s->L, a, st);
     mark_end(s, st);
     if (rc) return rc;
     s->launches++;
@@ -602,7 +644,19 @@ int image_step(tti_sim* s, int slot, cudaStream_t st)
     const tti_sim_config& c = s->cfg;
     int rc;
     mark_begin(s, 2, st);
-    if (c.fused && (c.snap_precision != SNAP_F32 || fused_image_supported(s->L))) {
+    if (c.fused && c.scheme == 1) {
+        ImageArgs ia{};
+        ia.adj3 = s->w.pd;
+        ia.adj4 = s->w.qd;
+        ia.store = s->snaps;
+        ia.snap_prec = c.snap_precision;
+        ia.snap_scale = s->snap_scale + (size_t)slot * 4;
+        ia.nsnap = s->nslot;
+        ia.slot = slot;
+        ia.grad_vp = s->grad_vp;
+        rc = launch_t1_image(s->L, ia, st);
+        s->launches++;
+    } else if (c.fused && (c.snap_precision != SNAP_F32 || fused_image_supported(s->L))) {
         ImageArgs ia{};
         ia.adj1 = s->w.p;
         ia.adj2 = s->w.q;

@@ -115,3 +115,45 @@ def oracle_rtm(o, lay, m, ab, cfg, src, wavelet, rec, residual=None, adjoint=Tru
     out["grad_vp"] = gvp.reshape(lay.nz, lay.ny, lay.nx)
     out["grad_rho"] = grho.reshape(lay.nz, lay.ny, lay.nx)
     return out
+
+
+def oracle_rtm_t1(o, lay, m, ab, cfg, src, wavelet, rec, residual=None):
+    """RTM with the centred constant-density operator (scheme 1), composed
+    from the oracle's type1 restatement in the simulator's step order:
+    forward step: loop2, loop4, fwd_main_loop_2_1 (sponge form when the
+    sponge is on), source, receivers; adjoint step: residual injection,
+    adj_main_loop_2, loop2, loop4; Vp image (update_grad_loop) at snapshot
+    steps, then the simulator's Vp finalisation."""
+    dt = np.float32(cfg.dt)
+    h = (cfg.dx, cfg.dy, cfg.dz)
+    sponge = cfg.sponge_width > 0
+    f1, f2, f3, f4 = (lay.zeros() for _ in range(4))
+    nrec = len(rec)
+    traces = np.zeros((cfg.nt, nrec), np.float32)
+    snaps = {}
+    I = lay.interior
+    for n in range(cfg.nt):
+        o.loop2(lay, f1, f2, f3, f4, ab[0], ab[1], ab[2], dt)
+        if cfg.free_surface:
+            o.loop4(lay, f1, f2)
+        o.t1_fwd(lay, f3, f4, f1, f2, m, ab, dt, h, 1 if sponge else 0)
+        if src >= 0:
+            f3.flat[src] += np.float32(wavelet[n]) * dt
+            f4.flat[src] += np.float32(wavelet[n]) * dt
+        traces[n] = -(2 * f1.flat[rec] + f2.flat[rec]) / np.float32(3)
+        if n % cfg.xcorr_step == 0:
+            snaps[n] = (np.ascontiguousarray(f3[I].ravel()), np.ascontiguousarray(f4[I].ravel()))
+    res = (traces if residual is None else residual).astype(np.float32)
+    a1, a2, a3, a4 = (lay.zeros() for _ in range(4))
+    gvp = np.zeros(lay.nx * lay.ny * lay.nz, np.float32)
+    for n in range(cfg.nt - 1, -1, -1):
+        a3.flat[rec] += np.float32(-2.0 / 3.0) * res[n]
+        a4.flat[rec] += np.float32(-1.0 / 3.0) * res[n]
+        o.t1_adj(lay, a3, a4, a1, a2, m, ab, dt, h, sponge)
+        o.loop2(lay, a1, a2, a3, a4, ab[0], ab[1], ab[2], dt)
+        if cfg.free_surface:
+            o.loop4(lay, a1, a2)
+        if n % cfg.xcorr_step == 0:
+            o.t1_grad(lay, snaps[n][0], snaps[n][1], gvp, a3, a4)
+    o.finalize_vp_gradient(lay, m["m3"], gvp, np.float32(cfg.dt * cfg.xcorr_step))
+    return {"traces": traces, "f3": f3, "grad_vp": gvp.reshape(lay.nz, lay.ny, lay.nx)}

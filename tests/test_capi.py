@@ -109,3 +109,15 @@ def test_footprint_accounts_for_snapshots_and_checkpoints():
     assert no_snap < ck
     # the reference kernel sequence needs its derivative volumes and scratch
     assert P.Config(**cfg, save_snapshots=False, fused=False).footprint_bytes() - no_snap == 14 * vol
+
+
+def test_scheme_is_validated_and_type1_needs_no_derivative_volumes():
+    base = dict(nx=64, ny=64, nz=64, nt=40, xcorr_step=4, save_snapshots=False)
+    for bad in (-1, 2):
+        with pytest.raises(P.TTIError) as e:
+            P.Config(**base, scheme=bad).footprint_bytes()
+        assert e.value.status == P.EINVAL
+    fused = P.Config(**base).footprint_bytes()
+    # the centred operator's kernel sequence works on p, q, pdot, qdot alone
+    assert P.Config(**base, scheme=1, fused=False).footprint_bytes() == fused
+    assert P.Config(**base, scheme=1).footprint_bytes() == fused
