@@ -35,6 +35,12 @@ METRIC = "TTI fwd+adj+grad Gpts/s & HBM % of peak; shots/hr, p50/p99 at fixed im
 # snapshot step; the fused kernels' per-launch figure is 64 B/pt.
 B_FWD, B_ADJ, B_IMG, B_SNAP = 64, 64, 16, 8
 B_VTI = 52  # forward or adjoint step on a VTI model: rx, ry, rz are not read
+# Centred constant-density operator (--scheme 1), per interior point: a
+# forward or adjoint step reads p, q, m1..m4, rx, ry, rz and pdot, qdot and
+# writes pdot, qdot and the next p, q: 60 B (48 on a VTI model); the Vp image
+# reads two snapshot fields and the adjoint pdot, qdot and updates the image:
+# 2*elt + 16 B per imaging step; the snapshot writes 2*elt B.
+B_T1, B_T1_VTI = 60, 48
 
 
 def parse():
@@ -49,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--per-kernel", action="store_true", help="reference kernel sequence instead of fused")
+    ap.add_argument("--scheme", type=int, choices=[0, 1], default=0,
+                    help="0: staggered variable-density operator; 1: centred constant-density (type1)")
     ap.add_argument("--snap-precision", choices=["fp32", "fp16", "bf16"], default="fp32",
                     help="snapshot storage (the stencils and time update stay FP32)")
     ap.add_argument("--checkpoint", type=int, default=0,
@@ -103,8 +111,9 @@ def workload(args, rank):
     src = (nx // 2 + (rank * 17) % max(1, nx // 4), ny // 2, 5)
     rec = EM.receiver_plane(nx, ny, 3)
     gname = f"{nx}^3" if nx == ny == nz else f"{nx}x{ny}x{nz}"
+    op = ", centred constant-density operator" if args.scheme == 1 else ""
     desc = {
-        "workload": (f"TTI RTM shot {gname}, dx={args.dx:g}m, sponge 24, {args.nt} steps, imaging every "
+        "workload": (f"TTI RTM shot {gname}{op}, dx={args.dx:g}m, sponge 24, {args.nt} steps, imaging every "
                      f"{args.xcorr}"),
         "grid": [nx, ny, nz], "nt": args.nt, "xcorr_step": args.xcorr, "sponge_width": 24, "dx": args.dx,
         "model": mdesc, "source": f"{args.f0:g} Hz Ricker", "receivers": f"{nx * ny} (plane z=3)",
@@ -158,6 +167,40 @@ def ncu_traffic():
 
 
 # ---------------------------------------------------------------------------
+def cpu_sample_t1(args, o, lay, m, ab, dt, st, nsteps):
+    """The oracle's type1 restatement in the simulator's step order (forward:
+    loop2, loop4, fwd_main_loop_2_1 in the sponge form; adjoint:
+    adj_main_loop_2, loop2, loop4; one Vp image), extrapolated to a shot."""
+    n = args.n
+    h = (10.0, 10.0, 10.0)
+    f1, f2, f3, f4 = st["f1"], st["f2"], st["f3"], st["f4"]
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        o.loop2(lay, f1, f2, f3, f4, ab[0], ab[1], ab[2], dt)
+        o.loop4(lay, f1, f2)
+        o.t1_fwd(lay, f3, f4, f1, f2, m, ab, dt, h, 1)
+    t_fwd = (time.perf_counter() - t0) / nsteps
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        o.t1_adj(lay, f3, f4, f1, f2, m, ab, dt, h, True)
+        o.loop2(lay, f1, f2, f3, f4, ab[0], ab[1], ab[2], dt)
+        o.loop4(lay, f1, f2)
+    t_adj = (time.perf_counter() - t0) / nsteps
+    s3 = np.ascontiguousarray(f3[lay.interior].ravel())
+    gvp = np.zeros(n * n * n, np.float32)
+    t0 = time.perf_counter()
+    o.t1_grad(lay, s3, s3, gvp, f3, f4)
+    t_img = time.perf_counter() - t0
+    t_shot = args.nt * (t_fwd + t_adj) + (args.nt // args.xcorr) * t_img
+    pts = float(n) ** 3 * args.nt
+    return {
+        "value": pts / t_shot / 1e9, "unit": "Gpts/s", "cores": o.num_threads(), "kind": "port",
+        "sample": (f"oracle type1 FP32 on {n}^3: {nsteps} forward + {nsteps} adjoint steps + 1 imaging step, "
+                   f"extrapolated to {args.nt} steps ({t_fwd:.2f}s/fwd, {t_adj:.2f}s/adj, {t_img:.3f}s/img)"),
+        "shot_s": t_shot,
+    }
+
+
 def cpu_sample(args, model_np, dt, nsteps=2):
     """The oracle (C restatement of the reference kernels, OpenMP on all host
     cores) on the same grid: nsteps forward steps, nsteps adjoint steps and one
@@ -184,6 +227,8 @@ def cpu_sample(args, model_np, dt, nsteps=2):
     g = o.grid(lay, np.float32(dt), (10.0, 10.0, 10.0), free_surface=True, sponge_active=True)
     st = new_state(lay)
     st["f1"][lay.interior] = np.random.default_rng(0).standard_normal((n, n, n)).astype(np.float32)
+    if getattr(args, "scheme", 0) == 1:
+        return cpu_sample_t1(args, o, lay, m, ab, np.float32(dt), st, nsteps)
     t0 = time.perf_counter()
     for _ in range(nsteps):
         o.fwd_step(g, st, m, ab)
@@ -260,7 +305,8 @@ def run_ours(args):
     npts = float(nx) * ny * nz
     cfg = P.Config(nx=nx, ny=ny, nz=nz, dx=args.dx, dy=args.dx, dz=args.dx, dt=dt, nt=args.nt,
                    xcorr_step=args.xcorr, sponge_width=24, free_surface=True, fused=not args.per_kernel,
-                   save_snapshots=True, snap_precision=args.snap_precision, checkpoint_every=args.checkpoint)
+                   save_snapshots=True, snap_precision=args.snap_precision, checkpoint_every=args.checkpoint,
+                   scheme=args.scheme)
     sim = P.Simulator(cfg)
     sim.set_source(*src, w)
     sim.set_receivers(rec)
@@ -272,7 +318,8 @@ def run_ours(args):
     sim.set_model(**model)
     tuned = None
     if args.bz:
-        for kind, b in zip(("forward", "adjoint", "imaging"), args.bz):
+        kinds = ("type1_forward", "type1_adjoint") if args.scheme == 1 else ("forward", "adjoint", "imaging")
+        for kind, b in zip(kinds, args.bz):
             P.tune_set(nx, ny, nz, kind, b)
         tuned = {k: {"bz": b} for k, b in zip(("forward", "adjoint", "imaging"), args.bz)}
     elif not args.per_kernel and not args.no_autotune:
@@ -333,17 +380,25 @@ def run_ours(args):
     kms, kn = times[kind]
     per_launch_s = (kms / max(kn, 1)) / 1e3
     vti = args.model == "layered"
-    b_step = B_VTI if vti else (B_FWD if kind == "forward" else B_ADJ)
+    t1 = args.scheme == 1
+    if t1:
+        b_step = B_T1_VTI if vti else B_T1
+    else:
+        b_step = B_VTI if vti else (B_FWD if kind == "forward" else B_ADJ)
     alg_bytes = b_step * npts
     achieved = alg_bytes / per_launch_s / 1e9 if kn else None
-    traffic = ncu_traffic().get(f"{kind}_dram_bytes_per_launch_{nx}x{ny}x{nz}")
-    roofline = {"kernel": f"fused {kind} step", "bound": "hbm", "achieved": achieved, "peak": peak,
+    traffic = ncu_traffic().get(f"{'type1_' if t1 else ''}{kind}_dram_bytes_per_launch_{nx}x{ny}x{nz}")
+    roofline = {"kernel": f"fused {'type1 ' if t1 else ''}{kind} step", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                 "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
                 "avg_launch_ms": per_launch_s * 1e3, "launches": kn}
     passes = {k: {"total_ms": v[0] / args.steps, "launches_per_shot": v[1] / args.steps}
               for k, v in times.items()}
-    step_bytes = ((2 * B_VTI if vti else B_FWD + B_ADJ) + B_IMG / args.xcorr + B_SNAP / args.xcorr) * npts
+    if t1:
+        elt = {"fp32": 4, "fp16": 2, "bf16": 2}[args.snap_precision]
+        step_bytes = (2 * b_step + (2 * elt + 16) / args.xcorr + 2 * elt / args.xcorr) * npts
+    else:
+        step_bytes = ((2 * B_VTI if vti else B_FWD + B_ADJ) + B_IMG / args.xcorr + B_SNAP / args.xcorr) * npts
     hbm_frac = step_bytes * args.nt / (ms_per_step / 1e3) / 1e9 / peak
 
     # end to end through the host-buffer API
@@ -384,6 +439,8 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, see config)",
         "config": {**desc, "parallelism": f"shot-parallel x{ws}" if ws > 1 else "single GPU",
                    "path": "reference kernel sequence" if args.per_kernel else "fused step kernels",
+                   "operator": ("centred constant-density (type1 kernels)" if args.scheme == 1
+                                else "staggered variable-density (type2 kernels)"),
                    "snapshots": args.snap_precision,
                    "work_split": ({k: v["bz"] for k, v in tuned.items() if isinstance(v, dict)}
                                   if tuned else "modelled")},

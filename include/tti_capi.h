@@ -313,7 +313,8 @@ int tti_selfcheck_bounded_wait(double seconds, tti_stream_t stream);
  * afterwards are unspecified (forward and adjoint start from zero).  The
  * split changes only the launch shape: results do not depend on bz. */
 typedef struct {
-    int bz[3];         /* chosen bz: forward, adjoint, imaging (0: not tuned) */
+    int bz[3];         /* chosen bz: forward, adjoint, imaging (0: not tuned); with scheme = 1
+                          the centred forward and adjoint kernels, imaging not tuned */
     float ms[3];       /* per-launch time at the chosen bz */
     float model_ms[3]; /* per-launch time at the wave-count model's bz */
     int ncand;         /* candidates tried per kernel */
@@ -321,7 +322,8 @@ typedef struct {
 int tti_sim_autotune(tti_sim* sim, int reps, tti_tune_report* out);
 
 /* Record (bz > 0) or clear (bz = 0) the planes per CTA used for kernel kind
- * (0 forward, 1 adjoint, 2 imaging) on an nx*ny*nz grid, current device;
+ * (0 forward, 1 adjoint, 2 imaging of the staggered scheme; 3 forward,
+ * 4 adjoint of the centred scheme) on an nx*ny*nz grid, current device;
  * tti_tune_get returns the bz in effect (recorded or modelled). */
 int tti_tune_set(int nx, int ny, int nz, int kind, int bz);
 int tti_tune_get(int nx, int ny, int nz, int kind);

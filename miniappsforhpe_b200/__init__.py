@@ -437,7 +437,9 @@ class Simulator:
 
     def autotune(self, reps: int = 3) -> dict:
         """Time every z-chunk candidate of the fused kernels on this grid and
-        record the fastest (include/tti_capi.h, tti_sim_autotune)."""
+        record the fastest (include/tti_capi.h, tti_sim_autotune).  With the
+        centred scheme the 'forward' and 'adjoint' entries are its type1
+        kernels."""
         r = TuneReport()
         self._chk(lib().tti_sim_autotune(self._h, int(reps), C.byref(r)), "tti_sim_autotune")
         kinds = ("forward", "adjoint", "imaging")
@@ -478,17 +480,20 @@ class Simulator:
         return int(lib().tti_sim_stream(self._h) or 0)
 
 
+TUNE_KINDS = ("forward", "adjoint", "imaging", "type1_forward", "type1_adjoint")
+
+
 def tune_set(nx: int, ny: int, nz: int, kind: str, bz: int) -> None:
     """Record (bz > 0) or clear (bz = 0) the z-chunk of a fused kernel kind
-    ('forward' | 'adjoint' | 'imaging') on an nx*ny*nz grid (current device)."""
-    k = ("forward", "adjoint", "imaging").index(kind)
+    (TUNE_KINDS) on an nx*ny*nz grid (current device)."""
+    k = TUNE_KINDS.index(kind)
     rc = lib().tti_tune_set(nx, ny, nz, k, bz)
     if rc != OK:
         raise TTIError(rc, "tti_tune_set")
 
 
 def tune_get(nx: int, ny: int, nz: int, kind: str) -> int:
-    k = ("forward", "adjoint", "imaging").index(kind)
+    k = TUNE_KINDS.index(kind)
     v = lib().tti_tune_get(nx, ny, nz, k)
     if v < 0:
         raise TTIError(-v, "tti_tune_get")

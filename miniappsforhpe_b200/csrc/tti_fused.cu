@@ -1384,7 +1384,7 @@ __global__ void __launch_bounds__(NT, 1)
         for (int s = 0; s < T1_NS; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
-    unsigned tmax[4] = {0u, 0u, 0u, 0u};
+    unsigned tmax[2] = {0u, 0u};
     int s = 0;
     uint32_t phase = 0;
     int gbase = 0;
@@ -1414,7 +1414,7 @@ __global__ void __launch_bounds__(NT, 1)
             }
             mbar_wait(&bars[s], phase, a.err, dead);
             const int z = zs - T1_LAG + t - T1_LAG;  // output plane
-            float snapv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            float snapv[2] = {0.0f, 0.0f};
             if (z >= zs && owner) {
                 const int64_t gi = L.idx(x, y, z);
                 const float a1 = __ldg(a.m1 + gi), a2 = __ldg(a.m2 + gi), a3 = __ldg(a.m3 + gi),
@@ -1453,16 +1453,14 @@ __global__ void __launch_bounds__(NT, 1)
                 a.f4[gi] = n4;
                 const float* C = ring + (size_t)back(T1_LAG) * 2 * IH * IW;
                 const float pc = C[vr * IW + vc], qc = C[IH * IW + vr * IW + vc];
-                if (a.snap) {
+                if (a.snap) {  // two-field slot: pdot, qdot (all the type1 image reads)
                     const int64_t nin = (int64_t)L.nx() * L.ny() * L.nz();
                     const int64_t dd = ((int64_t)(z - L.izbeg) * L.ny() + (y - L.iybeg)) * L.nx() + (x - L.ixbeg);
                     snapv[0] = n3;
                     snapv[1] = n4;
-                    snapv[2] = pc;
-                    snapv[3] = qc;
                     bool sat = false;
 #pragma unroll
-                    for (int f = 0; f < 4; ++f) {
+                    for (int f = 0; f < 2; ++f) {
                         const float sc = (a.snap_prec == SNAP_F32) ? 1.0f : a.snap_scale[f];
                         sat |= snap_store(a.snap, f * nin + dd, snapv[f] * sc, a.snap_prec);
                     }
@@ -1484,7 +1482,7 @@ __global__ void __launch_bounds__(NT, 1)
                 }
             }
 #pragma unroll
-            for (int f = 0; f < 4; ++f) tmax[f] = max(tmax[f], __float_as_uint(fabsf(snapv[f])));
+            for (int f = 0; f < 2; ++f) tmax[f] = max(tmax[f], __float_as_uint(fabsf(snapv[f])));
             if (++s == T1_NS) {
                 s = 0;
                 phase ^= 1u;
@@ -1493,7 +1491,7 @@ __global__ void __launch_bounds__(NT, 1)
     }  // segments
     if (a.snap && a.snap_prec != SNAP_F32) {
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
+        for (int f = 0; f < 2; ++f) {
             const unsigned m = __reduce_max_sync(0xffffffffu, tmax[f]);
             if ((tid & 31) == 0 && m) atomicMax(a.snap_amax + f, m);
         }
@@ -1911,7 +1909,7 @@ std::vector<int> plane_candidates(const Layout& L)
 // per SM (shared memory bound), each segment pays the 2*LAG-plane pipeline
 // fill, a range of bz planes covers at most ceil((bz-1)/nz)+1 columns (one
 // when whole columns divide evenly).
-double plane_cost(const Layout& L, int bz)
+double plane_cost(const Layout& L, int bz, int lag)
 {
     const int nz = L.nz();
     const long long ctas = cta_count(L, bz);
@@ -1924,7 +1922,7 @@ double plane_cost(const Layout& L, int bz)
         segs = bz / nz;
     else
         segs = (bz - 1) / nz + 2;
-    return waves * (bz + 2.0 * LAG * segs);
+    return waves * (bz + 2.0 * lag * segs);
 }
 
 // Column-aligned shares (bz divides nz): every CTA works down whole chunks
@@ -1940,9 +1938,11 @@ int pick_bz(const Layout& L, int kind)
 {
     int best = L.nz();
     double best_cost = 1e300;
+    const bool any_split = kind == KIND_FWD || kind == KIND_T1F;  // few staged arrays
+    const int lag = (kind == KIND_T1F || kind == KIND_T1A) ? T1_LAG : LAG;
     for (int bz : plane_candidates(L)) {
-        if (kind != KIND_FWD && !column_aligned(L, bz)) continue;
-        const double cost = plane_cost(L, bz);
+        if (!any_split && !column_aligned(L, bz)) continue;
+        const double cost = plane_cost(L, bz, lag);
         if (cost < best_cost - 1e-9) {
             best_cost = cost;
             best = bz;
@@ -2169,7 +2169,7 @@ int launch_t1_fused_forward(const Layout& L, const FwdStepArgs& s, int sponge, c
     a.src_index = s.src_index;
     a.src_term = s.src_term;
     a.L = L;
-    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_FWD);
+    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_T1F);
     a.fs = s.free_surface;
     a.sponge = sponge;
     a.dt = s.dt;
@@ -2203,7 +2203,7 @@ int launch_t1_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t 
     a.aby = s.aby;
     a.abz = s.abz;
     a.L = L;
-    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_ADJ);
+    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_T1A);
     a.fs = s.free_surface;
     a.sponge = s.sponge_active;
     a.dt = s.dt;
@@ -2225,7 +2225,7 @@ int launch_t1_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     if (s.snap_prec != SNAP_F32 && !s.snap_scale) return TTI_EINVAL;
     const int64_t nin = (int64_t)L.nx() * L.ny() * L.nz();
     const size_t elt = snap_elt_bytes(s.snap_prec);
-    const unsigned char* s3 = static_cast<const unsigned char*>(s.store) + (size_t)s.slot * 4 * nin * elt;
+    const unsigned char* s3 = static_cast<const unsigned char*>(s.store) + (size_t)s.slot * 2 * nin * elt;
     const unsigned char* s4 = s3 + (size_t)nin * elt;
     const float* sc = s.snap_prec == SNAP_F32 ? nullptr : s.snap_scale;
     const int blocks = (int)std::min<int64_t>((nin + 255) / 256, 148LL * 16);

@@ -118,7 +118,9 @@ int fused_wait_status(cudaStream_t st, int* word = nullptr);
 // this grid: each CTA takes that many consecutive planes of the grid's
 // (tile, z) planes in tile-major order.  The autotuned value if one was
 // recorded, else the wave-count model's.
-enum { KIND_FWD = 0, KIND_ADJ = 1, KIND_IMG = 2 };
+// kernel kinds of the work-split table: the staggered scheme's three fused
+// kernels, then the centred (type1) forward and adjoint step kernels
+enum { KIND_FWD = 0, KIND_ADJ = 1, KIND_IMG = 2, KIND_T1F = 3, KIND_T1A = 4, KIND_COUNT = 5 };
 int choose_bz(const Layout& L, int kind);
 void record_tuned_bz(const Layout& L, int kind, int bz);
 int tuned_bz(const Layout& L, int kind);  // 0 if none recorded

@@ -75,8 +75,10 @@ __global__ void k_snapshot_save(float* __restrict__ slot, const float* __restric
     int64_t v = L.idx(jx + L.ixbeg, jy + L.iybeg, jz + L.izbeg);
     slot[d] = f3[v];
     slot[n + d] = f4[v];
-    slot[2 * n + d] = f1[v];
-    slot[3 * n + d] = f2[v];
+    if (f1) {  // two-field slots (centred scheme) keep pdot and qdot only
+        slot[2 * n + d] = f1[v];
+        slot[3 * n + d] = f2[v];
+    }
 }
 
 __global__ void k_add_source(float* f3, float* f4, int64_t i, float term)
@@ -154,6 +156,11 @@ inline int cuda_rc(cudaError_t e)
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? TTI_ENOMEM : TTI_ELAUNCH;
 }
+
+// Fields per snapshot slot: pdot, qdot, p, q for the staggered scheme (its
+// density image differentiates the stored p/q); pdot and qdot alone for the
+// centred scheme, whose Vp image is all it makes.
+inline int snap_fields(const tti_sim_config& c) { return c.scheme == 1 ? 2 : 4; }
 
 } // namespace
 
@@ -237,7 +244,10 @@ struct tti_sim {
     }
     int64_t nvol() const { return (int64_t)L.ldimx * L.ldimy * L.ldimz; }
     dim3 dense_grid() const { return dim3((L.nx() + 127) / 128, L.ny(), L.nz()); }
-    size_t slot_bytes() const { return (size_t)4 * ninterior * snap_elt_bytes(cfg.snap_precision); }
+    size_t slot_bytes() const
+    {
+        return (size_t)snap_fields(cfg) * ninterior * snap_elt_bytes(cfg.snap_precision);
+    }
     void* slot_ptr(int k) const { return static_cast<unsigned char*>(snaps) + (size_t)k * slot_bytes(); }
 };
 
@@ -298,7 +308,8 @@ Plan plan_of(const tti_sim_config& c)
             pl.ckpts = (size_t)pl.ncp * 4 * nin * sizeof(float) + (size_t)pl.ncp * 4 * sizeof(unsigned int);
             pl.recompute = 6 * vb;
         }
-        pl.snaps = (size_t)pl.nslot * 4 * nin * snap_elt_bytes(c.snap_precision) + (size_t)pl.nslot * 4 * sizeof(float) +
+        pl.snaps = (size_t)pl.nslot * snap_fields(c) * nin * snap_elt_bytes(c.snap_precision) +
+                   (size_t)pl.nslot * 4 * sizeof(float) +
                    4 * sizeof(unsigned int);
     }
     return pl;
@@ -1031,8 +1042,10 @@ int tti_sim_forward(tti_sim* s, float* traces, int traces_on_device)
             if (!fused) {
                 if ((r = forward_per_kernel_step(s, n, st))) return r;
                 if (slot >= 0) {
+                    const bool two = snap_fields(c) == 2;
                     k_snapshot_save<<<s->dense_grid(), 128, 0, st>>>(static_cast<float*>(s->slot_ptr(slot)), s->w.pd,
-                                                                     s->w.qd, s->w.p, s->w.q, s->L);
+                                                                     s->w.qd, two ? nullptr : s->w.p,
+                                                                     two ? nullptr : s->w.q, s->L);
                     s->launches++;
                 }
                 if ((r = receivers_step(s, s->w, n, st))) return r;
@@ -1316,7 +1329,9 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
     *out = tti_tune_report{};
     const Layout& L = s->L;
     const tti_sim_config& c = s->cfg;
-    const bool img = s->snaps && (c.snap_precision != SNAP_F32 || fused_image_supported(L));
+    const bool t1 = c.scheme == 1;
+    // the type1 image is a point-wise kernel with no work split to tune
+    const bool img = !t1 && s->snaps && (c.snap_precision != SNAP_F32 || fused_image_supported(L));
     const std::vector<int> cand = bz_candidates(L);
     out->ncand = (int)cand.size();
     cudaStream_t st = s->stream;
@@ -1353,7 +1368,7 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
             a.dz = c.dz;
             a.err = s->err;
             a.bz = bz;
-            return launch_fused_forward(L, a, st);
+            return t1 ? launch_t1_fused_forward(L, a, s->sponge_active ? 1 : 0, st) : launch_fused_forward(L, a, st);
         }
         if (kind == KIND_ADJ) {
             AdjStepArgs a{};
@@ -1376,7 +1391,7 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
             a.dz = c.dz;
             a.err = s->err;
             a.bz = bz;
-            return launch_fused_adjoint(L, a, st);
+            return t1 ? launch_t1_fused_adjoint(L, a, st) : launch_fused_adjoint(L, a, st);
         }
         ImageArgs ia{};
         ia.adj1 = w.p;
@@ -1404,6 +1419,7 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
     if (s->snap_scale) rc = sim_zero(s, s->snap_scale, (size_t)s->nslot * 4 * sizeof(float));
     for (int kind = 0; kind < 3 && !rc; ++kind) {
         if (kind == KIND_IMG && !img) continue;
+        const int table_kind = !t1 ? kind : (kind == KIND_FWD ? KIND_T1F : KIND_T1A);
         float best = 1e30f;
         int best_bz = 0;
         for (int bz : cand) {
@@ -1416,14 +1432,14 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
             float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
             ms /= reps;
-            if (bz == model_bz(L, kind)) out->model_ms[kind] = ms;
+            if (bz == model_bz(L, table_kind)) out->model_ms[kind] = ms;
             if (ms < best) {
                 best = ms;
                 best_bz = bz;
             }
         }
         if (rc) break;
-        record_tuned_bz(L, kind, best_bz);
+        record_tuned_bz(L, table_kind, best_bz);
         out->bz[kind] = best_bz;
         out->ms[kind] = best;
     }
@@ -1449,7 +1465,7 @@ int tti_selfcheck_bounded_wait(double seconds, tti_stream_t stream)
 
 int tti_tune_set(int nx, int ny, int nz, int kind, int bz)
 {
-    if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind > 2 || bz < 0) return TTI_EINVAL;
+    if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind >= KIND_COUNT || bz < 0) return TTI_EINVAL;
     tti_sim_config c{};
     c.nx = nx;
     c.ny = ny;
@@ -1460,7 +1476,7 @@ int tti_tune_set(int nx, int ny, int nz, int kind, int bz)
 
 int tti_tune_get(int nx, int ny, int nz, int kind)
 {
-    if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind > 2) return -TTI_EINVAL;
+    if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind >= KIND_COUNT) return -TTI_EINVAL;
     tti_sim_config c{};
     c.nx = nx;
     c.ny = ny;

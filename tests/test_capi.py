@@ -121,3 +121,13 @@ def test_scheme_is_validated_and_type1_needs_no_derivative_volumes():
     # the centred operator's kernel sequence works on p, q, pdot, qdot alone
     assert P.Config(**base, scheme=1, fused=False).footprint_bytes() == fused
     assert P.Config(**base, scheme=1).footprint_bytes() == fused
+
+
+def test_type1_snapshot_slots_hold_two_fields():
+    n = 64 * 64 * 64
+    cfg = dict(nx=64, ny=64, nz=64, nt=400, xcorr_step=4, scheme=1)
+    none = P.Config(**cfg, save_snapshots=False).footprint_bytes()
+    for prec, elt in (("fp32", 4), ("fp16", 2)):
+        full = P.Config(**cfg, snap_precision=prec).footprint_bytes()
+        # 100 slots of pdot and qdot, their scales, the running maxima
+        assert full - none == 100 * (2 * n * elt + 16) + 16
