@@ -71,6 +71,8 @@ def parse():
                     help="use the modelled work split instead of timing the candidates first")
     ap.add_argument("--bz", type=int, nargs=3, default=None, metavar=("FWD", "ADJ", "IMG"),
                     help="fixed planes per CTA of the forward, adjoint and imaging kernels (implies --no-autotune)")
+    ap.add_argument("--ztop", type=int, nargs=3, default=[0, 0, 0], metavar=("FWD", "ADJ", "IMG"),
+                    help="with --bz: top/bottom split depth per kernel (0: plain tile-major split)")
     ap.add_argument("--serve", action="store_true",
                     help="served batch: Poisson stream of RTM shots through the shot server, "
                          "against the same stream run one shot at a time in plain FP32")
@@ -319,9 +321,9 @@ def run_ours(args):
     tuned = None
     if args.bz:
         kinds = ("type1_forward", "type1_adjoint") if args.scheme == 1 else ("forward", "adjoint", "imaging")
-        for kind, b in zip(kinds, args.bz):
-            P.tune_set(nx, ny, nz, kind, b)
-        tuned = {k: {"bz": b} for k, b in zip(("forward", "adjoint", "imaging"), args.bz)}
+        for kind, b, zt in zip(kinds, args.bz, args.ztop):
+            P.tune_set(nx, ny, nz, kind, b, zt)
+        tuned = {k: {"bz": b, "ztop": zt} for k, b, zt in zip(kinds[:2] + ("imaging",), args.bz, args.ztop)}
     elif not args.per_kernel and not args.no_autotune:
         tuned = sim.autotune(reps=2)  # outside the timed region; picks the work split per kernel
     gvp = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev)
@@ -442,7 +444,8 @@ def run_ours(args):
                    "operator": ("centred constant-density (type1 kernels)" if args.scheme == 1
                                 else "staggered variable-density (type2 kernels)"),
                    "snapshots": args.snap_precision,
-                   "work_split": ({k: v["bz"] for k, v in tuned.items() if isinstance(v, dict)}
+                   "work_split": ({k.replace("type1_", ""): [v["bz"], v.get("ztop", 0)]
+                                   for k, v in tuned.items() if isinstance(v, dict)}
                                   if tuned else "modelled")},
         "roofline": roofline, "hbm_frac_alg_per_step": hbm_frac,
         "shots_per_hour": 3600.0 * 1e3 / ms_per_step * ws,

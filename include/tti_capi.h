@@ -304,8 +304,10 @@ int tti_selfcheck_bounded_wait(double seconds, tti_stream_t stream);
  * split among CTAs in tile-major order, bz consecutive planes per CTA (one
  * or more column segments, each paying a pipeline fill of 14 planes), so bz
  * sets how many CTAs a step launches against the fill overhead.
- * tti_sim_autotune times every candidate bz (whole-column chunks ceil(nz/n)
- * and equal shares for 1..8 CTAs per SM, at least 8 planes) of the fused
+ * tti_sim_autotune times every candidate split (whole-column chunks
+ * ceil(nz/n), equal shares for 1..8 CTAs per SM of at least 8 planes, and,
+ * on grids with fewer tile columns than SMs, top/bottom splits as for
+ * tti_tune_set_split around the balance point of the tops) of the fused
  * forward, adjoint and (with a snapshot store) imaging kernels on this
  * simulator's volumes, reps launches each, and records the fastest for this
  * grid on the current device; later launches on any simulator of the same
@@ -315,6 +317,7 @@ int tti_selfcheck_bounded_wait(double seconds, tti_stream_t stream);
 typedef struct {
     int bz[3];         /* chosen bz: forward, adjoint, imaging (0: not tuned); with scheme = 1
                           the centred forward and adjoint kernels, imaging not tuned */
+    int ztop[3];       /* chosen top/bottom split (0: plain tile-major bz) */
     float ms[3];       /* per-launch time at the chosen bz */
     float model_ms[3]; /* per-launch time at the wave-count model's bz */
     int ncand;         /* candidates tried per kernel */
@@ -327,6 +330,12 @@ int tti_sim_autotune(tti_sim* sim, int reps, tti_tune_report* out);
  * tti_tune_get returns the bz in effect (recorded or modelled). */
 int tti_tune_set(int nx, int ny, int nz, int kind, int bz);
 int tti_tune_get(int nx, int ny, int nz, int kind);
+/* The same with a top/bottom split: ztop > 0 gives each of the grid's T
+ * tile columns a CTA for its top ztop planes and lets further CTAs share
+ * the columns' bottoms (planes ztop .. nz-1), bz planes each; ztop = 0 is
+ * the plain tile-major split of tti_tune_set. */
+int tti_tune_set_split(int nx, int ny, int nz, int kind, int bz, int ztop);
+int tti_tune_get_split(int nx, int ny, int nz, int kind, int* bz, int* ztop);
 
 /* Image readback: Vp gradient (finalised, -2*dt*xcorr/vp) and rho gradient,
  * nx*ny*nz each, host or device memory. */

@@ -62,7 +62,7 @@ class SimConfig(C.Structure):
 
 
 class TuneReport(C.Structure):
-    _fields_ = [("bz", I * 3), ("ms", F * 3), ("model_ms", F * 3), ("ncand", I)]
+    _fields_ = [("bz", I * 3), ("ztop", I * 3), ("ms", F * 3), ("model_ms", F * 3), ("ncand", I)]
 
 
 _SIGS = {
@@ -96,6 +96,8 @@ _SIGS = {
     "tti_sim_kernel_times": [V, V, V],
     "tti_sim_autotune": [V, I, C.POINTER(TuneReport)],
     "tti_tune_set": [I, I, I, I, I],
+    "tti_tune_set_split": [I, I, I, I, I, I],
+    "tti_tune_get_split": [I, I, I, I, V, V],
     "tti_selfcheck_bounded_wait": [D, V],
     "tti_tune_get": [I, I, I, I],
     "tti_sim_volume": [V, I, C.POINTER(V)],
@@ -443,8 +445,8 @@ class Simulator:
         r = TuneReport()
         self._chk(lib().tti_sim_autotune(self._h, int(reps), C.byref(r)), "tti_sim_autotune")
         kinds = ("forward", "adjoint", "imaging")
-        return {k: {"bz": r.bz[i], "ms": r.ms[i], "model_ms": r.model_ms[i]} for i, k in enumerate(kinds)
-                if r.bz[i] > 0} | {"candidates": r.ncand}
+        return {k: {"bz": r.bz[i], "ztop": r.ztop[i], "ms": r.ms[i], "model_ms": r.model_ms[i]}
+                for i, k in enumerate(kinds) if r.bz[i] > 0} | {"candidates": r.ncand}
 
     def image(self, out_vp=None, out_rho=None):
         """(grad_vp, grad_rho), each (nz, ny, nx); CUDA tensors if given."""
@@ -483,13 +485,14 @@ class Simulator:
 TUNE_KINDS = ("forward", "adjoint", "imaging", "type1_forward", "type1_adjoint")
 
 
-def tune_set(nx: int, ny: int, nz: int, kind: str, bz: int) -> None:
-    """Record (bz > 0) or clear (bz = 0) the z-chunk of a fused kernel kind
-    (TUNE_KINDS) on an nx*ny*nz grid (current device)."""
+def tune_set(nx: int, ny: int, nz: int, kind: str, bz: int, ztop: int = 0) -> None:
+    """Record (bz > 0) or clear (bz = 0) the work split of a fused kernel
+    kind (TUNE_KINDS) on an nx*ny*nz grid (current device); ztop > 0 is a
+    top/bottom split (tti_tune_set_split)."""
     k = TUNE_KINDS.index(kind)
-    rc = lib().tti_tune_set(nx, ny, nz, k, bz)
+    rc = lib().tti_tune_set_split(nx, ny, nz, k, bz, ztop)
     if rc != OK:
-        raise TTIError(rc, "tti_tune_set")
+        raise TTIError(rc, "tti_tune_set_split")
 
 
 def tune_get(nx: int, ny: int, nz: int, kind: str) -> int:
@@ -498,6 +501,15 @@ def tune_get(nx: int, ny: int, nz: int, kind: str) -> int:
     if v < 0:
         raise TTIError(-v, "tti_tune_get")
     return v
+
+
+def tune_get_split(nx: int, ny: int, nz: int, kind: str) -> tuple:
+    """(bz, ztop) of the split in effect for a kernel kind on this grid."""
+    bz, zt = I(), I()
+    rc = lib().tti_tune_get_split(nx, ny, nz, TUNE_KINDS.index(kind), C.byref(bz), C.byref(zt))
+    if rc != OK:
+        raise TTIError(rc, "tti_tune_get_split")
+    return bz.value, zt.value
 
 
 class SnapshotStore:

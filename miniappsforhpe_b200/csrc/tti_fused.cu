@@ -108,30 +108,41 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 struct Segment {
     int x0, y0, zs, len;
 };
+// With ztop > 0 the sequence is split in two: CTA t < tiles takes the top
+// ztop planes of column t; the other CTAs walk the columns' bottoms (planes
+// ztop .. nz-1 of every column, tile-major), per_cta planes each.
 struct WorkRange {
     long long pos, end;
-    int tiles_x, nz, ixbeg, iybeg, izbeg;
-    __device__ WorkRange(const Layout& L, int per_cta)
+    int tiles_x, span, zbase, ixbeg, iybeg, izbeg;
+    __device__ WorkRange(const Layout& L, int per_cta, int ztop)
     {
         tiles_x = (L.nx() + TX - 1) / TX;
-        const int tiles_y = (L.ny() + TY - 1) / TY;
-        nz = L.nz();
+        const long long tiles = (long long)tiles_x * ((L.ny() + TY - 1) / TY);
         ixbeg = L.ixbeg;
         iybeg = L.iybeg;
         izbeg = L.izbeg;
-        const long long W = (long long)tiles_x * tiles_y * nz;
-        pos = (long long)blockIdx.x * per_cta;
-        end = min(W, pos + per_cta);
+        long long cta = blockIdx.x;
+        if (ztop > 0 && cta < tiles) {
+            span = ztop;
+            zbase = 0;
+            per_cta = ztop;
+        } else {
+            span = L.nz() - ztop;
+            zbase = ztop;
+            if (ztop > 0) cta -= tiles;
+        }
+        pos = cta * per_cta;
+        end = min(tiles * span, pos + per_cta);
     }
     __device__ bool next(Segment& sg)
     {
         if (pos >= end) return false;
-        const long long tile = pos / nz;
-        const int z0 = (int)(pos - tile * nz);
-        sg.len = (int)min((long long)(nz - z0), end - pos);
+        const long long tile = pos / span;
+        const int z0 = (int)(pos - tile * span);
+        sg.len = (int)min((long long)(span - z0), end - pos);
         sg.x0 = ixbeg + (int)(tile % tiles_x) * TX;
         sg.y0 = iybeg + (int)(tile / tiles_x) * TY;
-        sg.zs = izbeg + z0;
+        sg.zs = izbeg + zbase + z0;
         pos += sg.len;
         return true;
     }
@@ -186,7 +197,8 @@ struct FwdParams {
     int64_t src_index;
     float src_term;
     Layout L;
-    int bz;  // z planes per chunk
+    int bz;    // planes per CTA (of the bottoms when ztop > 0)
+    int ztop;  // > 0: top/bottom split
     int fs;
     float dt, invdx, invdy, invdz, invdxdy, invdydz, invdzdx;
     int* err;
@@ -228,7 +240,7 @@ __global__ void __launch_bounds__(NT, 1)
     int gbase = 0;                        // planes consumed by earlier segments
     // This CTA's share of the (tile, z) work in tile-major order: a.bz planes
     // from blockIdx.x * a.bz, as one or more segments of a tile column.
-    WorkRange wr(L, a.bz);
+    WorkRange wr(L, a.bz, a.ztop);
     for (Segment sg; wr.next(sg); gbase += sg.len + 2 * LAG) {
     const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
     const int ntot = sg.len + 2 * LAG;  // arrival planes zs-7 .. ze+7
@@ -551,6 +563,7 @@ struct AdjParams {
     const float2 *abx, *aby, *abz;
     Layout L;
     int bz;
+    int ztop;
     int fs;
     int sponge;
     float dt, invdx, invdy, invdz, invdxy, invdyz, invdzx;
@@ -637,7 +650,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
     int s = 0;
     uint32_t phase = 0;
     int gbase = 0;  // planes consumed by earlier segments
-    WorkRange wr(L, a.bz);
+    WorkRange wr(L, a.bz, a.ztop);
     for (Segment sg; wr.next(sg); gbase += sg.len + 2 * LAG) {
     const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
     const int ntot = sg.len + 2 * LAG;
@@ -949,6 +962,7 @@ struct ImgParams {
     float *gvp, *grho;           // dense images
     Layout L;
     int bz;
+    int ztop;
     int fs;
     int slot;                    // snapshot index in the store
     float hx, hy, hz;
@@ -1036,7 +1050,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
     int s = 0;
     uint32_t phase = 0;
     int gbase = 0;  // planes consumed by earlier segments
-    WorkRange wr(L, a.bz);
+    WorkRange wr(L, a.bz, a.ztop);
     for (Segment sg; wr.next(sg); gbase += sg.len + 2 * LAG) {
     const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
     const int xd0 = x0 - L.ixbeg, yd0 = y0 - L.iybeg;  // dense (interior) origin
@@ -1316,6 +1330,7 @@ struct T1FwdParams {
     float src_term;
     Layout L;
     int bz;
+    int ztop;
     int fs;
     int sponge;  // 1: pdot = A pdot + B dt rhs (the launcher's use_sponge)
     float dt;
@@ -1388,7 +1403,7 @@ __global__ void __launch_bounds__(NT, 1)
     int s = 0;
     uint32_t phase = 0;
     int gbase = 0;
-    WorkRange wr(L, a.bz);
+    WorkRange wr(L, a.bz, a.ztop);
     for (Segment sg; wr.next(sg); gbase += sg.len + 2 * T1_LAG) {
         const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
         const int ntot = sg.len + 2 * T1_LAG;  // arrival planes zs-4 .. ze+4
@@ -1526,6 +1541,7 @@ struct T1AdjParams {
     const float2 *abx, *aby, *abz;
     Layout L;
     int bz;
+    int ztop;
     int fs;
     int sponge;
     float dt;
@@ -1565,7 +1581,7 @@ __global__ void __launch_bounds__(NT, 1) k_t1_fused_adjoint(const __grid_constan
     int s = 0;
     uint32_t phase = 0;
     int gbase = 0;
-    WorkRange wr(L, a.bz);
+    WorkRange wr(L, a.bz, a.ztop);
     for (Segment sg; wr.next(sg); gbase += sg.len + 2 * T1_LAG) {
         const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
         const int ntot = sg.len + 2 * T1_LAG;
@@ -1879,8 +1895,15 @@ long long work_planes(const Layout& L)
     return (long long)((L.nx() + TX - 1) / TX) * ((L.ny() + TY - 1) / TY) * L.nz();
 }
 
-// CTAs of a launch with bz planes per CTA.
-unsigned cta_count(const Layout& L, int bz) { return (unsigned)((work_planes(L) + bz - 1) / bz); }
+long long tile_count(const Layout& L) { return (long long)((L.nx() + TX - 1) / TX) * ((L.ny() + TY - 1) / TY); }
+
+// CTAs of a launch with the given split.
+unsigned cta_count(const Layout& L, Split sp)
+{
+    if (sp.ztop <= 0) return (unsigned)((work_planes(L) + sp.bz - 1) / sp.bz);
+    const long long T = tile_count(L);
+    return (unsigned)(T + (T * (L.nz() - sp.ztop) + sp.bz - 1) / sp.bz);
+}
 
 // Planes per CTA worth trying: whole-column chunks ceil(nz/n), and shares
 // that give every SM one, two, ... equal parts of the work; at least 8.
@@ -1912,7 +1935,7 @@ std::vector<int> plane_candidates(const Layout& L)
 double plane_cost(const Layout& L, int bz, int lag)
 {
     const int nz = L.nz();
-    const long long ctas = cta_count(L, bz);
+    const long long ctas = cta_count(L, Split{bz, 0});
     const int sms = device_sms();
     const double waves = (double)((ctas + sms - 1) / sms);
     int segs;
@@ -1934,12 +1957,47 @@ double plane_cost(const Layout& L, int bz, int lag)
 // kernel three).
 bool column_aligned(const Layout& L, int bz) { return bz <= L.nz() && L.nz() % bz == 0; }
 
+// Modelled cost of a top/bottom split in one wave: the tops (one segment
+// each) against the bottom CTAs, whose bz planes cross at most
+// ceil((bz-1)/span)+1 column bottoms.
+double split_cost(const Layout& L, Split sp, int lag)
+{
+    const int span = L.nz() - sp.ztop;
+    const int segs = (sp.bz - 1) / span + 2;
+    return std::max(sp.ztop + 2.0 * lag, sp.bz + 2.0 * lag * segs);
+}
+
+int kind_lag(int kind) { return (kind == KIND_T1F || kind == KIND_T1A) ? T1_LAG : LAG; }
+
+// Top/bottom splits for grids with fewer columns than SMs: the balance point
+// ztop = T (nz + 2 lag) / S of the tops against S - T bottom CTAs, and
+// neighbours 8 and 16 planes either side.
+std::vector<Split> topbottom_candidates(const Layout& L, int kind)
+{
+    std::vector<Split> c;
+    const long long T = tile_count(L);
+    const int S = device_sms(), nz = L.nz();
+    if (T >= S || nz < 16) return c;
+    const int lag = kind_lag(kind);
+    const int z0 = (int)(T * (nz + 2LL * lag) / S);
+    for (int dz : {0, -8, 8, -16, 16}) {
+        const int zt = z0 + dz;
+        if (zt < 8 || zt > nz - 4) continue;
+        const long long bottoms = T * (long long)(nz - zt);
+        const int bz = (int)((bottoms + (S - T) - 1) / (S - T));
+        if (bz < 1) continue;
+        const Split sp{bz, zt};
+        if (std::find(c.begin(), c.end(), sp) == c.end()) c.push_back(sp);
+    }
+    return c;
+}
+
 int pick_bz(const Layout& L, int kind)
 {
     int best = L.nz();
     double best_cost = 1e300;
     const bool any_split = kind == KIND_FWD || kind == KIND_T1F;  // few staged arrays
-    const int lag = (kind == KIND_T1F || kind == KIND_T1A) ? T1_LAG : LAG;
+    const int lag = kind_lag(kind);
     for (int bz : plane_candidates(L)) {
         if (!any_split && !column_aligned(L, bz)) continue;
         const double cost = plane_cost(L, bz, lag);
@@ -1983,7 +2041,10 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.src_index = s.src_index;
     a.src_term = s.src_term;
     a.L = L;
-    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_FWD);
+    const Split sp = s.bz > 0 ? Split{s.bz, s.ztop} : choose_split(L, KIND_FWD);
+    if (!split_valid(L, sp)) return TTI_EINVAL;
+    a.bz = sp.bz;
+    a.ztop = sp.ztop;
     a.fs = s.free_surface;
     a.dt = s.dt;
     a.invdx = 1.0 / s.dx;
@@ -1994,7 +2055,7 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.invdzdx = 1.0 / (4 * s.dx * s.dz);
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
-    dim3 grid(cta_count(L, a.bz));
+    dim3 grid(cta_count(L, sp));
     if (!kernels_prepared()) return TTI_ELAUNCH;
     if (s.vti)
         k_fused_forward<false><<<grid, dim3(TX, TY), FWD_SMEM, st>>>(mp, mq, mi, a);
@@ -2022,7 +2083,10 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     a.aby = s.aby;
     a.abz = s.abz;
     a.L = L;
-    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_ADJ);
+    const Split sp = s.bz > 0 ? Split{s.bz, s.ztop} : choose_split(L, KIND_ADJ);
+    if (!split_valid(L, sp)) return TTI_EINVAL;
+    a.bz = sp.bz;
+    a.ztop = sp.ztop;
     a.fs = s.free_surface;
     a.sponge = s.sponge_active;
     a.dt = s.dt;
@@ -2035,7 +2099,7 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
     const bool tti = !s.vti;
-    dim3 grid(cta_count(L, a.bz));
+    dim3 grid(cta_count(L, sp));
     if (!kernels_prepared()) return TTI_ELAUNCH;
     if (!tti)
         k_fused_adjoint<false><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
@@ -2112,7 +2176,10 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     a.gvp = s.grad_vp;
     a.grho = s.grad_rho;
     a.L = L;
-    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_IMG);
+    const Split sp = s.bz > 0 ? Split{s.bz, s.ztop} : choose_split(L, KIND_IMG);
+    if (!split_valid(L, sp)) return TTI_EINVAL;
+    a.bz = sp.bz;
+    a.ztop = sp.ztop;
     a.fs = s.free_surface;
     a.slot = s.slot;
     a.hx = 1.0 / s.dx;
@@ -2120,7 +2187,7 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     a.hz = 1.0 / s.dz;
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
-    dim3 grid(cta_count(L, a.bz));
+    dim3 grid(cta_count(L, sp));
     const bool tti = !s.vti;
     if (!kernels_prepared()) return TTI_ELAUNCH;
     switch (s.snap_prec) {
@@ -2169,7 +2236,10 @@ int launch_t1_fused_forward(const Layout& L, const FwdStepArgs& s, int sponge, c
     a.src_index = s.src_index;
     a.src_term = s.src_term;
     a.L = L;
-    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_T1F);
+    const Split sp = s.bz > 0 ? Split{s.bz, s.ztop} : choose_split(L, KIND_T1F);
+    if (!split_valid(L, sp)) return TTI_EINVAL;
+    a.bz = sp.bz;
+    a.ztop = sp.ztop;
     a.fs = s.free_surface;
     a.sponge = sponge;
     a.dt = s.dt;
@@ -2177,7 +2247,7 @@ int launch_t1_fused_forward(const Layout& L, const FwdStepArgs& s, int sponge, c
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
     if (!kernels_prepared()) return TTI_ELAUNCH;
-    const dim3 grid(cta_count(L, a.bz));
+    const dim3 grid(cta_count(L, sp));
     if (s.vti)
         k_t1_fused_forward<false><<<grid, dim3(TX, TY), T1F_SMEM, st>>>(mp, mq, a);
     else
@@ -2203,7 +2273,10 @@ int launch_t1_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t 
     a.aby = s.aby;
     a.abz = s.abz;
     a.L = L;
-    a.bz = s.bz > 0 ? s.bz : choose_bz(L, KIND_T1A);
+    const Split sp = s.bz > 0 ? Split{s.bz, s.ztop} : choose_split(L, KIND_T1A);
+    if (!split_valid(L, sp)) return TTI_EINVAL;
+    a.bz = sp.bz;
+    a.ztop = sp.ztop;
     a.fs = s.free_surface;
     a.sponge = s.sponge_active;
     a.dt = s.dt;
@@ -2211,7 +2284,7 @@ int launch_t1_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t 
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
     if (!kernels_prepared()) return TTI_ELAUNCH;
-    const dim3 grid(cta_count(L, a.bz));
+    const dim3 grid(cta_count(L, sp));
     if (s.vti)
         k_t1_fused_adjoint<false><<<grid, dim3(TX, TY), T1A_SMEM, st>>>(tm, a);
     else
@@ -2296,7 +2369,7 @@ int wait_selfcheck(cudaStream_t st, long long limit_cycles)
 
 namespace {
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, int> g_tuned;  // (device, nx, ny, nz, kind) -> bz
+std::map<std::tuple<int, int, int, int, int>, Split> g_tuned;  // (device, nx, ny, nz, kind) -> split
 int current_device()
 {
     int dev = 0;
@@ -2305,32 +2378,44 @@ int current_device()
 }
 } // namespace
 
-void record_tuned_bz(const Layout& L, int kind, int bz)
+bool split_valid(const Layout& L, Split sp)
+{
+    if (sp.bz < 1 || sp.ztop < 0 || sp.ztop >= L.nz()) return false;
+    return sp.ztop == 0 || tile_count(L) < (long long)cta_count(L, sp);
+}
+
+void record_tuned_split(const Layout& L, int kind, Split sp)
 {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     const auto key = std::make_tuple(current_device(), L.nx(), L.ny(), L.nz(), kind);
-    if (bz > 0)
-        g_tuned[key] = bz;
+    if (sp.bz > 0)
+        g_tuned[key] = sp;
     else
         g_tuned.erase(key);
 }
 
-int tuned_bz(const Layout& L, int kind)
+Split tuned_split(const Layout& L, int kind)
 {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(std::make_tuple(current_device(), L.nx(), L.ny(), L.nz(), kind));
-    return it == g_tuned.end() ? 0 : it->second;
+    return it == g_tuned.end() ? Split{} : it->second;
 }
 
-int model_bz(const Layout& L, int kind) { return pick_bz(L, kind); }
+Split model_split(const Layout& L, int kind) { return Split{pick_bz(L, kind), 0}; }
 
-int choose_bz(const Layout& L, int kind)
+Split choose_split(const Layout& L, int kind)
 {
-    const int t = tuned_bz(L, kind);
-    return t > 0 ? t : pick_bz(L, kind);
+    const Split t = tuned_split(L, kind);
+    return t.bz > 0 ? t : model_split(L, kind);
 }
 
-std::vector<int> bz_candidates(const Layout& L) { return plane_candidates(L); }
+std::vector<Split> split_candidates(const Layout& L, int kind)
+{
+    std::vector<Split> c;
+    for (int bz : plane_candidates(L)) c.push_back(Split{bz, 0});
+    for (const Split& sp : topbottom_candidates(L, kind)) c.push_back(sp);
+    return c;
+}
 
 // Bounded-wait status of the fused kernels on the current device: 0 if no
 // wait gave up since the last call; the word is cleared.

@@ -58,6 +58,7 @@ struct FwdStepArgs {
     double dx, dy, dz;
     int* err = nullptr;  // error word of the bounded waits (nullptr: the device's)
     int bz = 0;          // planes per CTA of the tile-major (tile, z) work (0: tuned or modelled)
+    int ztop = 0;        // > 0: column tops of ztop planes, bz planes per CTA of the bottoms
 };
 int launch_fused_forward(const Layout& L, const FwdStepArgs& a, cudaStream_t st);
 
@@ -79,6 +80,7 @@ struct AdjStepArgs {
     double dx, dy, dz;
     int* err = nullptr;
     int bz = 0;
+    int ztop = 0;
 };
 int launch_fused_adjoint(const Layout& L, const AdjStepArgs& a, cudaStream_t st);
 
@@ -104,6 +106,7 @@ struct ImageArgs {
     double dx, dy, dz;
     int* err = nullptr;
     int bz = 0;
+    int ztop = 0;
 };
 bool fused_image_supported(const Layout& L);
 int launch_fused_image(const Layout& L, const ImageArgs& a, cudaStream_t st);
@@ -114,20 +117,30 @@ int launch_fused_image(const Layout& L, const ImageArgs& a, cudaStream_t st);
 // reads the device's shared word.
 int fused_wait_status(cudaStream_t st, int* word = nullptr);
 
-// Planes per CTA of a fused kernel (kind 0 forward, 1 adjoint, 2 imaging) on
-// this grid: each CTA takes that many consecutive planes of the grid's
-// (tile, z) planes in tile-major order.  The autotuned value if one was
-// recorded, else the wave-count model's.
+// Work split of a fused kernel on this grid.  ztop = 0: each CTA takes bz
+// consecutive planes of the grid's (tile, z) planes in tile-major order.
+// ztop > 0 (grids with fewer tile columns than SMs): CTA t < tiles takes the
+// top ztop planes of column t, and the remaining CTAs share the columns'
+// bottoms (planes ztop .. nz-1, tile-major) bz planes each, so that every SM
+// has work while the CTAs that run side by side stay at the same depth.
 // kernel kinds of the work-split table: the staggered scheme's three fused
 // kernels, then the centred (type1) forward and adjoint step kernels
 enum { KIND_FWD = 0, KIND_ADJ = 1, KIND_IMG = 2, KIND_T1F = 3, KIND_T1A = 4, KIND_COUNT = 5 };
-int choose_bz(const Layout& L, int kind);
-void record_tuned_bz(const Layout& L, int kind, int bz);
-int tuned_bz(const Layout& L, int kind);  // 0 if none recorded
-int model_bz(const Layout& L, int kind);  // the wave-count model's choice
-// Candidates the tuner tries: whole-column chunks ceil(nz/n) and equal
-// shares of the work for 1..8 CTAs per SM, each at least 8 planes.
-std::vector<int> bz_candidates(const Layout& L);
+struct Split {
+    int bz = 0;
+    int ztop = 0;
+    bool operator==(const Split& o) const { return bz == o.bz && ztop == o.ztop; }
+};
+bool split_valid(const Layout& L, Split s);
+// The autotuned split if one was recorded, else the wave-count model's.
+Split choose_split(const Layout& L, int kind);
+void record_tuned_split(const Layout& L, int kind, Split s);  // bz = 0 clears
+Split tuned_split(const Layout& L, int kind);                 // bz = 0 if none recorded
+Split model_split(const Layout& L, int kind);
+// Candidates the tuner tries: whole-column chunks ceil(nz/n), equal shares
+// of the work for 1..8 CTAs per SM (each at least 8 planes), and top/bottom
+// splits around the balance point of the kind's pipeline fill.
+std::vector<Split> split_candidates(const Layout& L, int kind);
 
 // Type1 scheme (constant density, centred second derivatives): fused forward
 // step (pdot update with the sponge form when sponge = 1, as the type1

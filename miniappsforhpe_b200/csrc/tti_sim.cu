@@ -1332,8 +1332,6 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
     const bool t1 = c.scheme == 1;
     // the type1 image is a point-wise kernel with no work split to tune
     const bool img = !t1 && s->snaps && (c.snap_precision != SNAP_F32 || fused_image_supported(L));
-    const std::vector<int> cand = bz_candidates(L);
-    out->ncand = (int)cand.size();
     cudaStream_t st = s->stream;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
@@ -1344,7 +1342,7 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
     // Each candidate runs on the simulator's own volumes; the wavefield and
     // image contents afterwards are unspecified (forward() and adjoint()
     // start from zero).
-    auto launch = [&](int kind, int bz) -> int {
+    auto launch = [&](int kind, Split sp) -> int {
         WaveState& w = s->w;
         if (kind == KIND_FWD) {
             FwdStepArgs a{};
@@ -1367,7 +1365,8 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
             a.dy = c.dy;
             a.dz = c.dz;
             a.err = s->err;
-            a.bz = bz;
+            a.bz = sp.bz;
+            a.ztop = sp.ztop;
             return t1 ? launch_t1_fused_forward(L, a, s->sponge_active ? 1 : 0, st) : launch_fused_forward(L, a, st);
         }
         if (kind == KIND_ADJ) {
@@ -1390,7 +1389,8 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
             a.dy = c.dy;
             a.dz = c.dz;
             a.err = s->err;
-            a.bz = bz;
+            a.bz = sp.bz;
+            a.ztop = sp.ztop;
             return t1 ? launch_t1_fused_adjoint(L, a, st) : launch_fused_adjoint(L, a, st);
         }
         ImageArgs ia{};
@@ -1412,7 +1412,8 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
         ia.dy = c.dy;
         ia.dz = c.dz;
         ia.err = s->err;
-        ia.bz = bz;
+        ia.bz = sp.bz;
+        ia.ztop = sp.ztop;
         return launch_fused_image(L, ia, st);
     };
     int rc = TTI_OK;
@@ -1421,26 +1422,30 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
         if (kind == KIND_IMG && !img) continue;
         const int table_kind = !t1 ? kind : (kind == KIND_FWD ? KIND_T1F : KIND_T1A);
         float best = 1e30f;
-        int best_bz = 0;
-        for (int bz : cand) {
-            if ((rc = launch(kind, bz))) break;  // warm-up
+        Split best_sp{};
+        const std::vector<Split> cand = split_candidates(L, table_kind);
+        const Split modelled = model_split(L, table_kind);
+        out->ncand = std::max(out->ncand, (int)cand.size());
+        for (const Split& sp : cand) {
+            if ((rc = launch(kind, sp))) break;  // warm-up
             cudaEventRecord(e0, st);
-            for (int r = 0; r < reps && !rc; ++r) rc = launch(kind, bz);
+            for (int r = 0; r < reps && !rc; ++r) rc = launch(kind, sp);
             cudaEventRecord(e1, st);
             if (rc) break;
             if ((rc = cuda_rc(cudaEventSynchronize(e1)))) break;
             float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
             ms /= reps;
-            if (bz == model_bz(L, table_kind)) out->model_ms[kind] = ms;
+            if (sp == modelled) out->model_ms[kind] = ms;
             if (ms < best) {
                 best = ms;
-                best_bz = bz;
+                best_sp = sp;
             }
         }
         if (rc) break;
-        record_tuned_bz(L, table_kind, best_bz);
-        out->bz[kind] = best_bz;
+        record_tuned_split(L, table_kind, best_sp);
+        out->bz[kind] = best_sp.bz;
+        out->ztop[kind] = best_sp.ztop;
         out->ms[kind] = best;
     }
     if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
@@ -1463,25 +1468,39 @@ int tti_selfcheck_bounded_wait(double seconds, tti_stream_t stream)
     return wait_selfcheck(reinterpret_cast<cudaStream_t>(stream), cycles);
 }
 
-int tti_tune_set(int nx, int ny, int nz, int kind, int bz)
+int tti_tune_set_split(int nx, int ny, int nz, int kind, int bz, int ztop)
 {
     if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind >= KIND_COUNT || bz < 0) return TTI_EINVAL;
     tti_sim_config c{};
     c.nx = nx;
     c.ny = ny;
     c.nz = nz;
-    record_tuned_bz(layout_of(c), kind, bz);
+    const Layout L = layout_of(c);
+    if (bz > 0 && !split_valid(L, Split{bz, ztop})) return TTI_EINVAL;
+    record_tuned_split(L, kind, Split{bz, bz > 0 ? ztop : 0});
+    return TTI_OK;
+}
+
+int tti_tune_set(int nx, int ny, int nz, int kind, int bz) { return tti_tune_set_split(nx, ny, nz, kind, bz, 0); }
+
+int tti_tune_get_split(int nx, int ny, int nz, int kind, int* bz, int* ztop)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind >= KIND_COUNT || !bz || !ztop) return TTI_EINVAL;
+    tti_sim_config c{};
+    c.nx = nx;
+    c.ny = ny;
+    c.nz = nz;
+    const Split sp = choose_split(layout_of(c), kind);
+    *bz = sp.bz;
+    *ztop = sp.ztop;
     return TTI_OK;
 }
 
 int tti_tune_get(int nx, int ny, int nz, int kind)
 {
-    if (nx < 1 || ny < 1 || nz < 1 || kind < 0 || kind >= KIND_COUNT) return -TTI_EINVAL;
-    tti_sim_config c{};
-    c.nx = nx;
-    c.ny = ny;
-    c.nz = nz;
-    return choose_bz(layout_of(c), kind);
+    int bz = 0, ztop = 0;
+    const int rc = tti_tune_get_split(nx, ny, nz, kind, &bz, &ztop);
+    return rc ? -rc : bz;
 }
 
 int tti_sim_source_gradient(tti_sim* s, float* host_out)

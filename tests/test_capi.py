@@ -131,3 +131,21 @@ def test_type1_snapshot_slots_hold_two_fields():
         full = P.Config(**cfg, snap_precision=prec).footprint_bytes()
         # 100 slots of pdot and qdot, their scales, the running maxima
         assert full - none == 100 * (2 * n * elt + 16) + 16
+
+
+def test_work_split_table_round_trip():
+    """The split table is host state: it records (bz, ztop) per grid and
+    kernel kind and rejects a top that leaves no bottoms."""
+    try:
+        P.tune_set(64, 48, 40, "adjoint", 3, 17)
+        assert P.tune_get_split(64, 48, 40, "adjoint") == (3, 17)
+        assert P.tune_get(64, 48, 40, "adjoint") == 3
+        P.tune_set(64, 48, 40, "type1_forward", 12)
+        assert P.tune_get_split(64, 48, 40, "type1_forward") == (12, 0)
+        for bad in ((4, 40), (4, -1)):
+            with pytest.raises(P.TTIError) as e:
+                P.tune_set(64, 48, 40, "forward", *bad)
+            assert e.value.status == P.EINVAL
+    finally:
+        for k in P.TUNE_KINDS:
+            P.tune_set(64, 48, 40, k, 0)
