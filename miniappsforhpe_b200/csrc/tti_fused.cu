@@ -1338,62 +1338,141 @@ struct T1FwdParams {
     int* err;
 };
 
-// Centred derivatives of one field at the thread's column of output plane z,
-// from the ring (plane z+ir in slot back(4-ir)).  Sums in the order of
-// compute_z_contributions / compute_xy_contributions
-// (kernel_type1_gpu_fwd.cu:150-232).
+// Centred second derivatives of one field at one point, scaled by the
+// finite-difference constants; sums in the order of compute_z_contributions /
+// compute_xy_contributions (kernel_type1_gpu_fwd.cu:150-232).
 struct T1Drv {
     float xx, yy, zz, xy, yz, zx;
 };
-template <bool TTI, typename Back>
-__device__ __forceinline__ T1Drv t1_derivs(const float* ring, int field, Back back, int vr, int vc, const T1Fd& k)
-{
-    T1Drv d;
-    float zz = 0.0f, zx = 0.0f, yz = 0.0f;
-#pragma unroll
-    for (int ir = -4; ir <= 4; ++ir) {
-        const float c = c2(ir < 0 ? -ir : ir);
-        const float* P = ring + (size_t)back(4 - ir) * 2 * IH * IW + field * IH * IW;
-        zz = zz + c * P[vr * IW + vc];
-        if (TTI && ir != 0) {
-            zx = zx + c * (P[vr * IW + vc + ir] - P[vr * IW + vc - ir]);
-            yz = yz + c * (P[(vr + ir) * IW + vc] - P[(vr - ir) * IW + vc]);
-        }
-    }
-    const float* P = ring + (size_t)back(4) * 2 * IH * IW + field * IH * IW;
-    const float f0 = P[vr * IW + vc];
-    float xx = c2(0) * f0, yy = c2(0) * f0, xy = 0.0f;
-#pragma unroll
-    for (int q = 1; q <= 4; ++q) {
-        const float c = c2(q);
-        xx += c * (P[vr * IW + vc + q] + P[vr * IW + vc - q]);
-        yy += c * (P[(vr + q) * IW + vc] + P[(vr - q) * IW + vc]);
-        if (TTI)
-            xy += c * (P[(vr + q) * IW + vc + q] - P[(vr + q) * IW + vc - q] + P[(vr - q) * IW + vc - q] -
-                       P[(vr - q) * IW + vc + q]);
-    }
-    d.xx = xx * k.xx;
-    d.yy = yy * k.yy;
-    d.zz = zz * k.zz;
-    d.xy = xy * k.xy;
-    d.yz = yz * k.yz;
-    d.zx = zx * k.zx;
-    return d;
-}
 
 // One fused type1 forward step: the launcher's operator and pdot/qdot update
 // (with the sponge form when a.sponge), the point source, the snapshot, then
 // the next step's loop2 and free surface, as k_fused_forward does for type2.
+// Each thread computes two x-neighbouring outputs (x0+2tx, x0+2tx+1) from
+// an 11-plane ring of p,q tiles (halo 4; plane z+ir in slot back(4-ir)),
+// reading it with 64-bit loads: an even column pair is one aligned float2, a
+// pair that starts on an odd column takes the halves of two.
+constexpr int T1X2_TX = TX / 2;  // 16 x 16 threads
+constexpr int T1X2_NT = T1X2_TX * TY;
+
+template <int OFF>
+__device__ __forceinline__ float2 t1_pair(const float* row, int vc)
+{
+    // (row[vc+OFF], row[vc+OFF+1]) with vc even
+    if constexpr ((OFF & 1) == 0) {
+        return *reinterpret_cast<const float2*>(row + vc + OFF);
+    } else {
+        const float2 lo = *reinterpret_cast<const float2*>(row + vc + OFF - 1);
+        const float2 hi = *reinterpret_cast<const float2*>(row + vc + OFF + 1);
+        return make_float2(lo.y, hi.x);
+    }
+}
+
+template <int IR, bool TTI, typename Back>
+__device__ __forceinline__ void t1x2_zterm(const float* ring, int field, Back back, int vr, int vc, float2& zz,
+                                           float2& zx, float2& yz)
+{
+    const float c = c2(IR < 0 ? -IR : IR);
+    const float* P = ring + (size_t)back(4 - IR) * 2 * IH * IW + field * IH * IW;
+    const float2 v = t1_pair<0>(P + vr * IW, vc);
+    zz.x = zz.x + c * v.x;
+    zz.y = zz.y + c * v.y;
+    if constexpr (TTI && IR != 0) {
+        const float2 xp = t1_pair<IR>(P + vr * IW, vc), xm = t1_pair<-IR>(P + vr * IW, vc);
+        zx.x = zx.x + c * (xp.x - xm.x);
+        zx.y = zx.y + c * (xp.y - xm.y);
+        const float2 yp = t1_pair<0>(P + (vr + IR) * IW, vc), ym = t1_pair<0>(P + (vr - IR) * IW, vc);
+        yz.x = yz.x + c * (yp.x - ym.x);
+        yz.y = yz.y + c * (yp.y - ym.y);
+    }
+}
+
+template <int Q, bool TTI>
+__device__ __forceinline__ void t1x2_xyterm(const float* P, int vr, int vc, const float (&w)[10], float2& xx,
+                                            float2& yy, float2& xy)
+{
+    const float c = c2(Q);
+    xx.x += c * (w[4 + Q] + w[4 - Q]);
+    xx.y += c * (w[5 + Q] + w[5 - Q]);
+    const float2 yp = t1_pair<0>(P + (vr + Q) * IW, vc), ym = t1_pair<0>(P + (vr - Q) * IW, vc);
+    yy.x += c * (yp.x + ym.x);
+    yy.y += c * (yp.y + ym.y);
+    if constexpr (TTI) {
+        const float2 pp = t1_pair<Q>(P + (vr + Q) * IW, vc), pm = t1_pair<-Q>(P + (vr + Q) * IW, vc);
+        const float2 mm = t1_pair<-Q>(P + (vr - Q) * IW, vc), mp = t1_pair<Q>(P + (vr - Q) * IW, vc);
+        xy.x += c * (pp.x - pm.x + mm.x - mp.x);
+        xy.y += c * (pp.y - pm.y + mm.y - mp.y);
+    }
+}
+
+struct T1Drv2 {
+    T1Drv a, b;
+};
+
+template <bool TTI, typename Back>
+__device__ __forceinline__ T1Drv2 t1x2_derivs(const float* ring, int field, Back back, int vr, int vc, const T1Fd& k)
+{
+    float2 zz = make_float2(0.0f, 0.0f), zx = zz, yz = zz;
+    t1x2_zterm<-4, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    t1x2_zterm<-3, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    t1x2_zterm<-2, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    t1x2_zterm<-1, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    t1x2_zterm<0, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    t1x2_zterm<1, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    t1x2_zterm<2, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    t1x2_zterm<3, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    t1x2_zterm<4, TTI>(ring, field, back, vr, vc, zz, zx, yz);
+    const float* P = ring + (size_t)back(4) * 2 * IH * IW + field * IH * IW;
+    float w[10];  // row vr, columns vc-4 .. vc+5
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        const float2 v = *reinterpret_cast<const float2*>(P + vr * IW + vc - 4 + 2 * j);
+        w[2 * j] = v.x;
+        w[2 * j + 1] = v.y;
+    }
+    float2 xx = make_float2(c2(0) * w[4], c2(0) * w[5]), yy = xx, xy = make_float2(0.0f, 0.0f);
+    t1x2_xyterm<1, TTI>(P, vr, vc, w, xx, yy, xy);
+    t1x2_xyterm<2, TTI>(P, vr, vc, w, xx, yy, xy);
+    t1x2_xyterm<3, TTI>(P, vr, vc, w, xx, yy, xy);
+    t1x2_xyterm<4, TTI>(P, vr, vc, w, xx, yy, xy);
+    T1Drv2 d;
+    d.a = T1Drv{xx.x * k.xx, yy.x * k.yy, zz.x * k.zz, xy.x * k.xy, yz.x * k.yz, zx.x * k.zx};
+    d.b = T1Drv{xx.y * k.xx, yy.y * k.yy, zz.y * k.zz, xy.y * k.xy, yz.y * k.yz, zx.y * k.zx};
+    return d;
+}
+
+// Operator of one point (compute_result, kernel_type1_gpu_fwd.cu:122-146).
 template <bool TTI>
-__global__ void __launch_bounds__(NT, 1)
-    k_t1_fused_forward(const __grid_constant__ CUtensorMap tm_p, const __grid_constant__ CUtensorMap tm_q,
-                       const T1FwdParams a)
+__device__ __forceinline__ void t1_rhs(const T1Drv& d1, const T1Drv& d2, float a1, float a2, float a3, float a4,
+                                       float vrx, float vry, float vrz, float& r3, float& r4)
+{
+    if constexpr (TTI) {
+        const float rxx = vrx * vrx, ryy = vry * vry, rzz = vrz * vrz;
+        const float rxy = 2.0f * vrx * vry, ryz = 2.0f * vry * vrz, rzx = 2.0f * vrz * vrx;
+        const float V1 = rxx * d1.xx + ryy * d1.yy + rzz * d1.zz + rxy * d1.xy + rzx * d1.zx + ryz * d1.yz;
+        const float H1 = d1.xx + d1.yy + d1.zz - V1;
+        const float V2 = rxx * d2.xx + ryy * d2.yy + rzz * d2.zz + rxy * d2.xy + rzx * d2.zx + ryz * d2.yz;
+        const float H2 = d2.xx + d2.yy + d2.zz - V2;
+        r3 = a1 * H1 + a4 * V1 + a2 * V2;
+        r4 = a2 * H1 + a3 * V2 + a4 * H2;
+    } else {
+        const float V1 = d1.zz, H1 = d1.xx + d1.yy + d1.zz - V1;
+        const float V2 = d2.zz, H2 = d2.xx + d2.yy + d2.zz - V2;
+        r3 = a1 * H1 + a4 * V1 + a2 * V2;
+        r4 = a2 * H1 + a3 * V2 + a4 * H2;
+    }
+}
+
+template <bool TTI>
+__global__ void __launch_bounds__(T1X2_NT, 2)
+    k_t1_fused_forward_x2(const __grid_constant__ CUtensorMap tm_p, const __grid_constant__ CUtensorMap tm_q,
+                          const T1FwdParams a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     float* ring = reinterpret_cast<float*>(smem);  // [NS][2][IH][IW]
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + T1_NS * T1_SLOT);
     const Layout& L = a.L;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * T1X2_TX + tx;
     bool dead = false;
     if (tid == 0) {
         for (int s = 0; s < T1_NS; ++s) mbar_init(&bars[s], 1);
@@ -1407,8 +1486,9 @@ __global__ void __launch_bounds__(NT, 1)
     for (Segment sg; wr.next(sg); gbase += sg.len + 2 * T1_LAG) {
         const int x0 = sg.x0, y0 = sg.y0, zs = sg.zs;
         const int ntot = sg.len + 2 * T1_LAG;  // arrival planes zs-4 .. ze+4
-        const int x = x0 + tx, y = y0 + ty;
-        const bool owner = (x <= L.ixend) && (y <= L.iyend);
+        const int xa = x0 + 2 * tx, y = y0 + ty;
+        const bool own_a = (xa <= L.ixend) && (y <= L.iyend);
+        const bool own_b = own_a && (xa + 1 <= L.ixend);
         __syncthreads();
         auto issue = [&](int t) {
             const int sl = (gbase + t) % T1_NS, z = zs - T1_LAG + t;
@@ -1419,7 +1499,7 @@ __global__ void __launch_bounds__(NT, 1)
         };
         if (tid == 0)
             for (int t = 0; t < T1_PF && t < ntot; ++t) issue(t);
-        const int vc = tx + 4, vr = ty + 4;
+        const int vc = 2 * tx + 4, vr = ty + 4;
         auto back = [&](int kk) { const int v = s - kk; return v < 0 ? v + T1_NS : v; };
         for (int t = 0; t < ntot; ++t) {
             __syncthreads();  // every thread is done with iteration t-1
@@ -1429,75 +1509,96 @@ __global__ void __launch_bounds__(NT, 1)
             }
             mbar_wait(&bars[s], phase, a.err, dead);
             const int z = zs - T1_LAG + t - T1_LAG;  // output plane
-            float snapv[2] = {0.0f, 0.0f};
-            if (z >= zs && owner) {
-                const int64_t gi = L.idx(x, y, z);
-                const float a1 = __ldg(a.m1 + gi), a2 = __ldg(a.m2 + gi), a3 = __ldg(a.m3 + gi),
-                            a4 = __ldg(a.m4 + gi);
-                const float vrx = TTI ? __ldg(a.rx + gi) : 0.0f, vry = TTI ? __ldg(a.ry + gi) : 0.0f,
-                            vrz = TTI ? __ldg(a.rz + gi) : 1.0f;
-                const float o3 = a.f3[gi], o4 = a.f4[gi];
-                const float2 sx = __ldg(a.abx + x), sy = __ldg(a.aby + y), sz = __ldg(a.abz + z);
-                const T1Drv d1 = t1_derivs<TTI>(ring, 0, back, vr, vc, a.k);
-                const T1Drv d2 = t1_derivs<TTI>(ring, 1, back, vr, vc, a.k);
-                float r3, r4;
+            float snapv[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
+            if (z >= zs && own_a) {
+                // the pair's point-wise values (x even, so every pair is 8-byte aligned)
+                const int64_t gi = L.idx(xa, y, z);
+                const float2 a1 = __ldg(reinterpret_cast<const float2*>(a.m1 + gi));
+                const float2 a2 = __ldg(reinterpret_cast<const float2*>(a.m2 + gi));
+                const float2 a3 = __ldg(reinterpret_cast<const float2*>(a.m3 + gi));
+                const float2 a4 = __ldg(reinterpret_cast<const float2*>(a.m4 + gi));
+                float2 vrx = make_float2(0.0f, 0.0f), vry = vrx, vrz = make_float2(1.0f, 1.0f);
                 if constexpr (TTI) {
-                    const float rxx = vrx * vrx, ryy = vry * vry, rzz = vrz * vrz;
-                    const float rxy = 2.0f * vrx * vry, ryz = 2.0f * vry * vrz, rzx = 2.0f * vrz * vrx;
-                    const float V1 = rxx * d1.xx + ryy * d1.yy + rzz * d1.zz + rxy * d1.xy + rzx * d1.zx + ryz * d1.yz;
-                    const float H1 = d1.xx + d1.yy + d1.zz - V1;
-                    const float V2 = rxx * d2.xx + ryy * d2.yy + rzz * d2.zz + rxy * d2.xy + rzx * d2.zx + ryz * d2.yz;
-                    const float H2 = d2.xx + d2.yy + d2.zz - V2;
-                    r3 = a1 * H1 + a4 * V1 + a2 * V2;
-                    r4 = a2 * H1 + a3 * V2 + a4 * H2;
-                } else {
-                    const float V1 = d1.zz, H1 = d1.xx + d1.yy + d1.zz - V1;
-                    const float V2 = d2.zz, H2 = d2.xx + d2.yy + d2.zz - V2;
-                    r3 = a1 * H1 + a4 * V1 + a2 * V2;
-                    r4 = a2 * H1 + a3 * V2 + a4 * H2;
+                    vrx = __ldg(reinterpret_cast<const float2*>(a.rx + gi));
+                    vry = __ldg(reinterpret_cast<const float2*>(a.ry + gi));
+                    vrz = __ldg(reinterpret_cast<const float2*>(a.rz + gi));
                 }
-                const float A = fminf(sx.x, fminf(sy.x, sz.x));
-                const float B = fminf(sx.y, fminf(sy.y, sz.y));
-                float n3 = a.sponge ? A * o3 + B * r3 * a.dt : o3 + r3 * a.dt;
-                float n4 = a.sponge ? A * o4 + B * r4 * a.dt : o4 + r4 * a.dt;
+                const float2 o3 = *reinterpret_cast<const float2*>(a.f3 + gi);
+                const float2 o4 = *reinterpret_cast<const float2*>(a.f4 + gi);
+                const float4 sx = __ldg(reinterpret_cast<const float4*>(a.abx + xa));
+                const float2 sy = __ldg(a.aby + y), sz = __ldg(a.abz + z);
+                const T1Drv2 d1 = t1x2_derivs<TTI>(ring, 0, back, vr, vc, a.k);
+                const T1Drv2 d2 = t1x2_derivs<TTI>(ring, 1, back, vr, vc, a.k);
+                float r3a, r4a, r3b, r4b;
+                t1_rhs<TTI>(d1.a, d2.a, a1.x, a2.x, a3.x, a4.x, vrx.x, vry.x, vrz.x, r3a, r4a);
+                t1_rhs<TTI>(d1.b, d2.b, a1.y, a2.y, a3.y, a4.y, vrx.y, vry.y, vrz.y, r3b, r4b);
+                const float Aa = fminf(sx.x, fminf(sy.x, sz.x)), Ba = fminf(sx.y, fminf(sy.y, sz.y));
+                const float Ab = fminf(sx.z, fminf(sy.x, sz.x)), Bb = fminf(sx.w, fminf(sy.y, sz.y));
+                float n3a = a.sponge ? Aa * o3.x + Ba * r3a * a.dt : o3.x + r3a * a.dt;
+                float n4a = a.sponge ? Aa * o4.x + Ba * r4a * a.dt : o4.x + r4a * a.dt;
+                float n3b = a.sponge ? Ab * o3.y + Bb * r3b * a.dt : o3.y + r3b * a.dt;
+                float n4b = a.sponge ? Ab * o4.y + Bb * r4b * a.dt : o4.y + r4b * a.dt;
                 if (gi == a.src_index) {
-                    n3 += a.src_term;
-                    n4 += a.src_term;
+                    n3a += a.src_term;
+                    n4a += a.src_term;
                 }
-                a.f3[gi] = n3;
-                a.f4[gi] = n4;
+                if (gi + 1 == a.src_index) {
+                    n3b += a.src_term;
+                    n4b += a.src_term;
+                }
                 const float* C = ring + (size_t)back(T1_LAG) * 2 * IH * IW;
-                const float pc = C[vr * IW + vc], qc = C[IH * IW + vr * IW + vc];
+                const float2 pc = *reinterpret_cast<const float2*>(C + vr * IW + vc);
+                const float2 qc = *reinterpret_cast<const float2*>(C + IH * IW + vr * IW + vc);
+                // next step's loop2 (kernel_base.cu:92-101) and free surface (:142-162)
+                float2 np = make_float2(Aa * pc.x + Ba * n3a * a.dt, Ab * pc.y + Bb * n3b * a.dt);
+                float2 nq = make_float2(Aa * qc.x + Ba * n4a * a.dt, Ab * qc.y + Bb * n4b * a.dt);
+                if (a.fs && z == L.izbeg) {
+                    np = make_float2(0.0f, 0.0f);
+                    nq = np;
+                }
+                const bool mirror = a.fs && z > L.izbeg && z <= L.izbeg + kRadius;
+                const int64_t gm = L.idx(xa, y, 2 * L.izbeg - z);
+                if (own_b) {
+                    *reinterpret_cast<float2*>(a.f3 + gi) = make_float2(n3a, n3b);
+                    *reinterpret_cast<float2*>(a.f4 + gi) = make_float2(n4a, n4b);
+                    *reinterpret_cast<float2*>(a.pout + gi) = np;
+                    *reinterpret_cast<float2*>(a.qout + gi) = nq;
+                    if (mirror) {
+                        *reinterpret_cast<float2*>(a.pout + gm) = make_float2(-np.x, -np.y);
+                        *reinterpret_cast<float2*>(a.qout + gm) = make_float2(-nq.x, -nq.y);
+                    }
+                } else {
+                    a.f3[gi] = n3a;
+                    a.f4[gi] = n4a;
+                    a.pout[gi] = np.x;
+                    a.qout[gi] = nq.x;
+                    if (mirror) {
+                        a.pout[gm] = -np.x;
+                        a.qout[gm] = -nq.x;
+                    }
+                }
                 if (a.snap) {  // two-field slot: pdot, qdot (all the type1 image reads)
                     const int64_t nin = (int64_t)L.nx() * L.ny() * L.nz();
-                    const int64_t dd = ((int64_t)(z - L.izbeg) * L.ny() + (y - L.iybeg)) * L.nx() + (x - L.ixbeg);
-                    snapv[0] = n3;
-                    snapv[1] = n4;
+                    const int64_t dd = ((int64_t)(z - L.izbeg) * L.ny() + (y - L.iybeg)) * L.nx() + (xa - L.ixbeg);
+                    snapv[0][0] = n3a;
+                    snapv[1][0] = n4a;
+                    if (own_b) {
+                        snapv[0][1] = n3b;
+                        snapv[1][1] = n4b;
+                    }
                     bool sat = false;
 #pragma unroll
                     for (int f = 0; f < 2; ++f) {
                         const float sc = (a.snap_prec == SNAP_F32) ? 1.0f : a.snap_scale[f];
-                        sat |= snap_store(a.snap, f * nin + dd, snapv[f] * sc, a.snap_prec);
+                        sat |= snap_store(a.snap, f * nin + dd, snapv[f][0] * sc, a.snap_prec);
+                        if (own_b) sat |= snap_store(a.snap, f * nin + dd + 1, snapv[f][1] * sc, a.snap_prec);
                     }
                     if (sat) atomicOr(a.err, 2);
                 }
-                // next step's loop2 (kernel_base.cu:92-101) and free surface (:142-162)
-                float np = A * pc + B * n3 * a.dt;
-                float nq = A * qc + B * n4 * a.dt;
-                if (a.fs && z == L.izbeg) {
-                    np = 0.0f;
-                    nq = 0.0f;
-                }
-                a.pout[gi] = np;
-                a.qout[gi] = nq;
-                if (a.fs && z > L.izbeg && z <= L.izbeg + kRadius) {
-                    const int64_t gm = L.idx(x, y, 2 * L.izbeg - z);
-                    a.pout[gm] = -np;
-                    a.qout[gm] = -nq;
-                }
             }
 #pragma unroll
-            for (int f = 0; f < 2; ++f) tmax[f] = max(tmax[f], __float_as_uint(fabsf(snapv[f])));
+            for (int f = 0; f < 2; ++f)
+                tmax[f] = max(tmax[f], max(__float_as_uint(fabsf(snapv[f][0])), __float_as_uint(fabsf(snapv[f][1]))));
             if (++s == T1_NS) {
                 s = 0;
                 phase ^= 1u;
@@ -1844,7 +1945,7 @@ bool prepare_device()
          set_smem(k_fused_image<true, __half>, img_smem(2));
     ok = ok && set_smem(k_fused_image<false, __nv_bfloat16>, img_smem(2)) &&
          set_smem(k_fused_image<true, __nv_bfloat16>, img_smem(2));
-    ok = ok && set_smem(k_t1_fused_forward<false>, T1F_SMEM) && set_smem(k_t1_fused_forward<true>, T1F_SMEM);
+    ok = ok && set_smem(k_t1_fused_forward_x2<false>, T1F_SMEM) && set_smem(k_t1_fused_forward_x2<true>, T1F_SMEM);
     ok = ok && set_smem(k_t1_fused_adjoint<false>, T1A_SMEM) && set_smem(k_t1_fused_adjoint<true>, T1A_SMEM);
     if (!ok) cudaGetLastError();
     return ok;
@@ -1976,18 +2077,21 @@ std::vector<Split> topbottom_candidates(const Layout& L, int kind)
 {
     std::vector<Split> c;
     const long long T = tile_count(L);
-    const int S = device_sms(), nz = L.nz();
-    if (T >= S || nz < 16) return c;
+    const int nz = L.nz();
     const int lag = kind_lag(kind);
-    const int z0 = (int)(T * (nz + 2LL * lag) / S);
-    for (int dz : {0, -8, 8, -16, 16}) {
-        const int zt = z0 + dz;
-        if (zt < 8 || zt > nz - 4) continue;
-        const long long bottoms = T * (long long)(nz - zt);
-        const int bz = (int)((bottoms + (S - T) - 1) / (S - T));
-        if (bz < 1) continue;
-        const Split sp{bz, zt};
-        if (std::find(c.begin(), c.end(), sp) == c.end()) c.push_back(sp);
+    // S: CTAs resident at once (one or two per SM)
+    for (int S : {device_sms(), 2 * device_sms()}) {
+        if (T >= S || nz < 16) continue;
+        const int z0 = (int)(T * (nz + 2LL * lag) / S);
+        for (int dz : {0, -8, 8, -16, 16}) {
+            const int zt = z0 + dz;
+            if (zt < 8 || zt > nz - 4) continue;
+            const long long bottoms = T * (long long)(nz - zt);
+            const int bz = (int)((bottoms + (S - T) - 1) / (S - T));
+            if (bz < 1) continue;
+            const Split sp{bz, zt};
+            if (std::find(c.begin(), c.end(), sp) == c.end()) c.push_back(sp);
+        }
     }
     return c;
 }
@@ -2249,9 +2353,9 @@ int launch_t1_fused_forward(const Layout& L, const FwdStepArgs& s, int sponge, c
     if (!kernels_prepared()) return TTI_ELAUNCH;
     const dim3 grid(cta_count(L, sp));
     if (s.vti)
-        k_t1_fused_forward<false><<<grid, dim3(TX, TY), T1F_SMEM, st>>>(mp, mq, a);
+        k_t1_fused_forward_x2<false><<<grid, dim3(T1X2_TX, TY), T1F_SMEM, st>>>(mp, mq, a);
     else
-        k_t1_fused_forward<true><<<grid, dim3(TX, TY), T1F_SMEM, st>>>(mp, mq, a);
+        k_t1_fused_forward_x2<true><<<grid, dim3(T1X2_TX, TY), T1F_SMEM, st>>>(mp, mq, a);
     return launch_status();
 }
 
