@@ -337,6 +337,33 @@ int tti_tune_get(int nx, int ny, int nz, int kind);
 int tti_tune_set_split(int nx, int ny, int nz, int kind, int bz, int ztop);
 int tti_tune_get_split(int nx, int ny, int nz, int kind, int* bz, int* ztop);
 
+/* Step-level calls for a caller that keeps its own time loop (the loop body
+ * of simulator2SetUp::execute, simulator2/simulator2SetUp.cu:517-814): the
+ * kernels of tti_sim_forward / tti_sim_adjoint, one time step per call,
+ * enqueued on the simulator's stream without synchronising.  Needs
+ * checkpoint_every = 0 and use_graphs = 0.  Calls out of order return
+ * TTI_ESTATE.
+ *   tti_sim_forward_begin: zero the wavefields (fused: and the step-0 p/q
+ *     update); then tti_sim_forward_step for n = 0 .. nt-1 in order: receiver
+ *     sample, the step, the snapshot at n % xcorr_step == 0;
+ *     tti_sim_get_traces reads the traces back (synchronises).
+ *   tti_sim_adjoint_begin: zero the adjoint wavefields and images and take
+ *     the residual traces (nt*nrec, as tti_sim_adjoint; NULL = zero); then
+ *     tti_sim_adjoint_step for n = nt-1 .. 0 in order (residual injection and
+ *     the adjoint step), each snapshot step n optionally followed by
+ *     tti_sim_image_step(n) (Vp and rho images from the stored snapshot);
+ *     tti_sim_adjoint_finish after step 0 finalises the Vp image,
+ *     synchronises and returns the bounded-wait status.
+ *   tti_sim_sync: synchronise the stream and return that status. */
+int tti_sim_forward_begin(tti_sim* sim);
+int tti_sim_forward_step(tti_sim* sim, int n);
+int tti_sim_get_traces(tti_sim* sim, float* traces, int on_device);
+int tti_sim_adjoint_begin(tti_sim* sim, const float* residual, int residual_on_device);
+int tti_sim_adjoint_step(tti_sim* sim, int n);
+int tti_sim_image_step(tti_sim* sim, int n);
+int tti_sim_adjoint_finish(tti_sim* sim);
+int tti_sim_sync(tti_sim* sim);
+
 /* Image readback: Vp gradient (finalised, -2*dt*xcorr/vp) and rho gradient,
  * nx*ny*nz each, host or device memory. */
 int tti_sim_get_image(tti_sim* sim, float* grad_vp, float* grad_rho, int on_device);
@@ -461,6 +488,14 @@ typedef struct {
     int max_resident;             /* most shots resident at once */
     double busy_ms;               /* device time of all rounds */
 } tti_server_stats;
+
+/* Run-level call: one whole shot from host arrays, synchronously, on a
+ * simulator created and destroyed for it (forward with receivers, adjoint
+ * driven by observed - synthetic traces, or by the synthetic traces when
+ * observed is NULL, images into image_vp / image_rho).  opts (NULL =
+ * defaults) contributes only fused, snap_precision, checkpoint_every,
+ * use_graphs and scheme; the physical set-up comes from the request. */
+int tti_rtm_shot(const tti_shot_request* req, const tti_sim_config* opts);
 
 int tti_server_create(const tti_server_config* cfg, tti_server** out);
 int tti_server_submit(tti_server* srv, const tti_shot_request* req, int64_t* ticket);

@@ -92,6 +92,14 @@ _SIGS = {
     "tti_sim_get_image": [V, V, V, I],
     "tti_sim_source_gradient": [V, V],
     "tti_sim_adjoint_observed": [V, V, I],
+    "tti_sim_forward_begin": [V],
+    "tti_sim_forward_step": [V, I],
+    "tti_sim_get_traces": [V, V, I],
+    "tti_sim_adjoint_begin": [V, V, I],
+    "tti_sim_adjoint_step": [V, I],
+    "tti_sim_image_step": [V, I],
+    "tti_sim_adjoint_finish": [V],
+    "tti_sim_sync": [V],
     "tti_sim_set_profiling": [V, I],
     "tti_sim_kernel_times": [V, V, V],
     "tti_sim_autotune": [V, I, C.POINTER(TuneReport)],
@@ -426,6 +434,36 @@ class Simulator:
             return
         o = np.ascontiguousarray(observed, np.float32).reshape(self.cfg.nt, self.nrec)
         self._chk(lib().tti_sim_adjoint_observed(self._h, o.ctypes.data_as(V), 0), "tti_sim_adjoint_observed")
+
+    # Step-level calls (tti_sim_forward_begin ... tti_sim_adjoint_finish): the
+    # same kernels as forward()/adjoint(), one time step per call.
+    def forward_begin(self):
+        self._chk(lib().tti_sim_forward_begin(self._h), "tti_sim_forward_begin")
+
+    def forward_step(self, n: int):
+        self._chk(lib().tti_sim_forward_step(self._h, int(n)), "tti_sim_forward_step")
+
+    def traces(self) -> np.ndarray:
+        out = np.zeros((self.cfg.nt, self.nrec), np.float32)
+        if self.nrec:
+            self._chk(lib().tti_sim_get_traces(self._h, out.ctypes.data_as(V), 0), "tti_sim_get_traces")
+        return out
+
+    def adjoint_begin(self, residual=None):
+        if residual is None:
+            self._chk(lib().tti_sim_adjoint_begin(self._h, None, 0), "tti_sim_adjoint_begin")
+            return
+        self._resid = np.ascontiguousarray(residual, np.float32).reshape(self.cfg.nt, self.nrec)
+        self._chk(lib().tti_sim_adjoint_begin(self._h, self._resid.ctypes.data_as(V), 0), "tti_sim_adjoint_begin")
+
+    def adjoint_step(self, n: int):
+        self._chk(lib().tti_sim_adjoint_step(self._h, int(n)), "tti_sim_adjoint_step")
+
+    def image_step(self, n: int):
+        self._chk(lib().tti_sim_image_step(self._h, int(n)), "tti_sim_image_step")
+
+    def adjoint_finish(self):
+        self._chk(lib().tti_sim_adjoint_finish(self._h), "tti_sim_adjoint_finish")
 
     def set_profiling(self, enable: bool):
         self._chk(lib().tti_sim_set_profiling(self._h, int(enable)), "tti_sim_set_profiling")

@@ -226,6 +226,9 @@ struct tti_sim {
     // resumable shot: phase 0 idle, 1 forward, 2 adjoint, 3 done
     int sh_phase = 0, sh_n = 0, sh_seg = 0;
     bool sh_recomp = false;
+    // step-level cursor: 0 idle, 1 forward (next step st_n), 2 adjoint (next
+    // step st_n, last adjoint step st_last, imaged st_imaged)
+    int st_mode = 0, st_n = 0, st_last = -1, st_imaged = -1;
 
     int alloc(void** p, size_t bytes)
     {
@@ -742,7 +745,7 @@ int restore_checkpoint(tti_sim* s, WaveState& w, int k, cudaStream_t st)
 // trace, residual injection, the step, and imaging at snapshot steps from
 // store slot (n - seg_start) / xcorr_step.  observed: s->resid holds observed
 // traces and the residual is formed from the last forward's traces.
-int adjoint_unit(tti_sim* s, int n, int seg_start, bool observed, cudaStream_t st)
+int adjoint_unit(tti_sim* s, int n, int seg_start, bool observed, cudaStream_t st, bool with_image = true)
 {
     const tti_sim_config& c = s->cfg;
     int r = TTI_OK;
@@ -761,7 +764,7 @@ int adjoint_unit(tti_sim* s, int n, int seg_start, bool observed, cudaStream_t s
     } else {
         if ((r = fused_adjoint_step(s, st))) return r;
     }
-    if (n % c.xcorr_step == 0 && (r = image_step(s, (n - seg_start) / c.xcorr_step, st))) return r;
+    if (with_image && n % c.xcorr_step == 0 && (r = image_step(s, (n - seg_start) / c.xcorr_step, st))) return r;
     return launch_status();
 }
 
@@ -1023,6 +1026,7 @@ int tti_sim_forward(tti_sim* s, float* traces, int traces_on_device)
     const tti_sim_config& c = s->cfg;
     s->launches = 0;
     s->forward_done = false;
+    s->st_mode = 0;
     int rc = zero_state(s, s->w);
     if (!rc && s->snap_amax) rc = sim_zero(s, s->snap_amax, 4 * sizeof(unsigned int));
     if (rc) return rc;
@@ -1094,6 +1098,7 @@ static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device
     const tti_sim_config& c = s->cfg;
     cudaStream_t st0 = s->stream;
     s->launches = 0;
+    s->st_mode = 0;
     int rc = zero_state(s, s->w);
     if (!rc) rc = sim_zero(s, s->grad_vp, s->ninterior * sizeof(float));
     if (!rc) rc = sim_zero(s, s->grad_rho, s->ninterior * sizeof(float));
@@ -1144,6 +1149,184 @@ static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device
     rc = cuda_rc(cudaStreamSynchronize(st0));
     if (!rc && fused) rc = fused_wait_status(st0, s->err);
     collect_marks(s);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Step-level calls (the loop body of simulator2SetUp::execute,
+// simulator2SetUp.cu:517-814, one time step per call).
+int tti_sim_forward_begin(tti_sim* s)
+{
+    if (!s) return TTI_EINVAL;
+    if (!s->model_set) return TTI_ESTATE;
+    if (s->cfg.checkpoint_every > 0 || s->cfg.use_graphs) return TTI_EINVAL;
+    s->launches = 0;
+    s->forward_done = false;
+    s->st_mode = 0;
+    int rc = zero_state(s, s->w);
+    if (!rc && s->snap_amax) rc = sim_zero(s, s->snap_amax, 4 * sizeof(unsigned int));
+    if (!rc && s->cfg.fused) rc = fused_prologue(s, s->w, s->stream);
+    if (rc) return rc;
+    s->st_mode = 1;
+    s->st_n = 0;
+    return TTI_OK;
+}
+
+int tti_sim_forward_step(tti_sim* s, int n)
+{
+    if (!s) return TTI_EINVAL;
+    if (s->st_mode != 1 || n != s->st_n) return TTI_ESTATE;
+    const tti_sim_config& c = s->cfg;
+    cudaStream_t st = s->stream;
+    const int slot = (c.save_snapshots && n % c.xcorr_step == 0) ? n / c.xcorr_step : -1;
+    int r = TTI_OK;
+    if (!c.fused) {
+        if ((r = forward_per_kernel_step(s, n, st))) return r;
+        if (slot >= 0) {
+            const bool two = snap_fields(c) == 2;
+            k_snapshot_save<<<s->dense_grid(), 128, 0, st>>>(static_cast<float*>(s->slot_ptr(slot)), s->w.pd,
+                                                             s->w.qd, two ? nullptr : s->w.p, two ? nullptr : s->w.q,
+                                                             s->L);
+            s->launches++;
+        }
+        if ((r = receivers_step(s, s->w, n, st))) return r;
+    } else {
+        if ((r = receivers_step(s, s->w, n, st))) return r;
+        if ((r = fused_forward_step(s, s->w, n, slot, st))) return r;
+    }
+    if ((r = launch_status())) return r;
+    if (++s->st_n == c.nt) {
+        s->st_mode = 0;
+        s->forward_done = true;
+    }
+    return TTI_OK;
+}
+
+int tti_sim_get_traces(tti_sim* s, float* traces, int on_device)
+{
+    if (!s || !traces) return TTI_EINVAL;
+    if (!s->nrec) return TTI_OK;
+    const size_t bytes = (size_t)s->nrec * s->cfg.nt * sizeof(float);
+    cudaError_t e = cudaMemcpyAsync(traces, s->traces, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                    s->stream);
+    if (e != cudaSuccess) return cuda_rc(e);
+    return cuda_rc(cudaStreamSynchronize(s->stream));
+}
+
+int tti_sim_adjoint_begin(tti_sim* s, const float* residual, int residual_on_device)
+{
+    if (!s) return TTI_EINVAL;
+    if (!s->model_set || !s->forward_done || !s->cfg.save_snapshots) return TTI_ESTATE;
+    if (s->cfg.checkpoint_every > 0 || s->cfg.use_graphs) return TTI_EINVAL;
+    const tti_sim_config& c = s->cfg;
+    s->launches = 0;
+    s->st_mode = 0;
+    int rc = zero_state(s, s->w);
+    if (!rc) rc = sim_zero(s, s->grad_vp, s->ninterior * sizeof(float));
+    if (!rc) rc = sim_zero(s, s->grad_rho, s->ninterior * sizeof(float));
+    if (!rc && s->nrec) {
+        if (residual) {
+            const size_t bytes = (size_t)s->nrec * c.nt * sizeof(float);
+            cudaError_t e = cudaMemcpyAsync(s->resid, residual, bytes,
+                                            residual_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                            s->stream);
+            if (e != cudaSuccess) rc = cuda_rc(e);
+        } else {
+            rc = sim_zero(s, s->resid, (size_t)s->nrec * c.nt * sizeof(float));
+        }
+    }
+    if (rc) return rc;
+    s->st_mode = 2;
+    s->st_n = c.nt - 1;
+    s->st_last = -1;
+    s->st_imaged = -1;
+    return TTI_OK;
+}
+
+int tti_sim_adjoint_step(tti_sim* s, int n)
+{
+    if (!s) return TTI_EINVAL;
+    if (s->st_mode != 2 || n != s->st_n) return TTI_ESTATE;
+    const int r = adjoint_unit(s, n, 0, false, s->stream, false);
+    if (r) return r;
+    s->st_last = n;
+    s->st_n = n - 1;
+    return TTI_OK;
+}
+
+int tti_sim_image_step(tti_sim* s, int n)
+{
+    if (!s) return TTI_EINVAL;
+    if (s->st_mode != 2 || n != s->st_last || s->st_imaged == n) return TTI_ESTATE;
+    if (n % s->cfg.xcorr_step != 0) return TTI_EINVAL;
+    const int r = image_step(s, n / s->cfg.xcorr_step, s->stream);
+    if (r) return r;
+    s->st_imaged = n;
+    return launch_status();
+}
+
+int tti_sim_adjoint_finish(tti_sim* s)
+{
+    if (!s) return TTI_EINVAL;
+    if (s->st_mode != 2 || s->st_n != -1) return TTI_ESTATE;
+    cudaStream_t st = s->stream;
+    k_finalize_dense<<<s->dense_grid(), 128, 0, st>>>(s->grad_vp, s->mv[3], s->L, s->cfg.dt * s->cfg.xcorr_step);
+    s->launches++;
+    s->st_mode = 0;
+    int rc = cuda_rc(cudaStreamSynchronize(st));
+    if (!rc && s->cfg.fused) rc = fused_wait_status(st, s->err);
+    collect_marks(s);
+    return rc;
+}
+
+int tti_sim_sync(tti_sim* s)
+{
+    if (!s) return TTI_EINVAL;
+    int rc = cuda_rc(cudaStreamSynchronize(s->stream));
+    if (!rc && s->cfg.fused) rc = fused_wait_status(s->stream, s->err);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Run-level call: one whole shot from host arrays.
+int tti_rtm_shot(const tti_shot_request* r, const tti_sim_config* opts)
+{
+    if (!r) return TTI_EINVAL;
+    tti_sim_config c{};
+    c.nx = r->nx;
+    c.ny = r->ny;
+    c.nz = r->nz;
+    c.dx = r->dx;
+    c.dy = r->dy;
+    c.dz = r->dz;
+    c.dt = r->dt;
+    c.nt = r->nt;
+    c.xcorr_step = r->xcorr_step;
+    c.sponge_width = r->sponge_width;
+    c.free_surface = r->free_surface;
+    c.fused = opts ? opts->fused : 1;
+    c.save_snapshots = 1;
+    c.snap_precision = opts ? opts->snap_precision : 0;
+    c.checkpoint_every = opts ? opts->checkpoint_every : 0;
+    c.use_graphs = opts ? opts->use_graphs : 0;
+    c.scheme = opts ? opts->scheme : 0;
+    tti_sim* s = nullptr;
+    int rc = tti_sim_create(&c, &s);
+    if (!rc) rc = tti_sim_set_model(s, r->vp, r->eps, r->delta, r->vs, r->theta, r->phi, r->rho);
+    if (!rc) rc = tti_sim_set_source(s, r->src_ix, r->src_iy, r->src_iz, r->wavelet, r->nt);
+    if (!rc) rc = tti_sim_set_receivers(s, r->nrec, r->rec_ixyz);
+    if (!rc) rc = tti_sim_forward(s, r->traces, 0);
+    if (!rc) {
+        if (r->observed)
+            rc = tti_sim_adjoint_observed(s, r->observed, 0);
+        else  // residual = the synthetic traces themselves
+            rc = tti_sim_adjoint(s, s->nrec ? s->traces : nullptr, 1);
+    }
+    if (!rc && (r->image_vp || r->image_rho)) rc = tti_sim_get_image(s, r->image_vp, r->image_rho, 0);
+    if (s) {
+        const int rd = tti_sim_destroy(s);
+        if (!rc) rc = rd;
+    }
     return rc;
 }
 

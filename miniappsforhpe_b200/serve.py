@@ -56,6 +56,8 @@ def _lib():
         l.tti_server_now.argtypes = [V]
         l.tti_server_now.restype = D
         l.tti_server_destroy.argtypes = [V]
+        l.tti_rtm_shot.argtypes = [C.POINTER(ShotRequestC), V]
+        l.tti_rtm_shot.restype = I
         for n in ("tti_server_create", "tti_server_submit", "tti_server_wait", "tti_server_stats_get",
                   "tti_server_destroy"):
             getattr(l, n).restype = I
@@ -145,6 +147,19 @@ class Result:
     @property
     def latency(self) -> float:
         return self.t_done - self.t_submit
+
+
+def rtm_shot(shot: Shot, opts=None) -> Shot:
+    """One whole shot, synchronously (tti_rtm_shot): fills ``shot.image_vp``,
+    ``shot.image_rho`` and ``shot.traces``.  ``opts`` is a
+    ``miniappsforhpe_b200.Config`` whose fused, snap_precision,
+    checkpoint_every, use_graphs and scheme fields are used (None: defaults)."""
+    req = shot._c()
+    cfg = opts.c_struct() if opts is not None else None
+    rc = _lib().tti_rtm_shot(C.byref(req), C.byref(cfg) if cfg is not None else None)
+    if rc != OK:
+        raise TTIError(rc, "tti_rtm_shot")
+    return shot
 
 
 class Server:
