@@ -487,6 +487,11 @@ typedef struct {
     int64_t graph_instantiations;
     int max_resident;             /* most shots resident at once */
     double busy_ms;               /* device time of all rounds */
+    double gap_ms;                /* device idle between a round and the one issued behind it
+                                     (the host was late with the next round) */
+    double build_ms;              /* host time spent capturing, updating and launching rounds */
+    double setup_ms;              /* host time spent admitting shots (allocation, model upload,
+                                     autotuning a new grid) */
 } tti_server_stats;
 
 /* Run-level call: one whole shot from host arrays, synchronously, on a

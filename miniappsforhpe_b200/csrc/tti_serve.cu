@@ -245,7 +245,12 @@ void loader_main(tti_server* srv)
             srv->resident += 1;
             sh->res.t_admit = srv->now();
         }
+        const double t_setup = srv->now();
         int rc = build_shot(srv, sh);
+        {
+            std::lock_guard<std::mutex> lk(srv->mu);
+            srv->stats.setup_ms += 1e3 * (srv->now() - t_setup);
+        }
         if (rc) {
             finish_shot(srv, sh, rc);
             continue;
@@ -355,12 +360,15 @@ void scheduler_main(tti_server* srv)
         // waits for the host between rounds
         int rc = TTI_OK;
         if (!plan.empty()) {
+            const double t_build = srv->now();
             rc = build_round(srv, plan, slot);
             if (!rc && srv->cfg.use_graphs) {
                 cudaEventRecord(srv->round_start[slot], srv->main);
                 rc = rc_of(cudaGraphLaunch(srv->exec[slot], srv->main));
             }
             if (!rc) rc = rc_of(cudaEventRecord(srv->round_end[slot], srv->main));
+            std::lock_guard<std::mutex> lk(srv->mu);
+            srv->stats.build_ms += 1e3 * (srv->now() - t_build);
         }
         // then wait for the round in flight and retire what it finished,
         // while round r+1 runs
@@ -370,6 +378,12 @@ void scheduler_main(tti_server* srv)
             if (cudaEventElapsedTime(&ms, srv->round_start[slot ^ 1], srv->round_end[slot ^ 1]) == cudaSuccess) {
                 std::lock_guard<std::mutex> lk(srv->mu);
                 srv->stats.busy_ms += ms;
+            }
+            // device gap between that round and the one just issued behind it
+            if (!plan.empty() && !rc && cudaEventSynchronize(srv->round_start[slot]) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, srv->round_end[slot ^ 1], srv->round_start[slot]) == cudaSuccess) {
+                std::lock_guard<std::mutex> lk(srv->mu);
+                srv->stats.gap_ms += std::max(0.0f, ms);
             }
             cudaGetLastError();
             for (Shot* s : inflight_finishing) {
