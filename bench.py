@@ -565,7 +565,8 @@ def serve_summary(recs, stats, stream):
             "device_busy_frac": stats["busy_ms"] / 1e3 / span, "rounds": stats["rounds"],
             "graph_updates": stats["graph_updates"], "graph_instantiations": stats["graph_instantiations"],
             "max_resident": stats["max_resident"], "device_gap_s": stats.get("gap_ms", 0.0) / 1e3,
-            "host_round_build_s": stats.get("build_ms", 0.0) / 1e3, "host_setup_s": stats.get("setup_ms", 0.0) / 1e3}
+            "host_round_build_s": stats.get("build_ms", 0.0) / 1e3, "host_setup_s": stats.get("setup_ms", 0.0) / 1e3,
+            "host_setup_split_s": {k: stats.get(f"setup_{k}_ms", 0.0) / 1e3 for k in ("alloc", "model", "tune")}}
 
 
 def run_serve(args):

@@ -492,6 +492,10 @@ typedef struct {
     double build_ms;              /* host time spent capturing, updating and launching rounds */
     double setup_ms;              /* host time spent admitting shots (allocation, model upload,
                                      autotuning a new grid) */
+    int max_batched;              /* most shots advanced in one round */
+    double setup_alloc_ms;        /* of setup_ms: creating the shots' simulators (device allocation) */
+    double setup_model_ms;        /* of setup_ms: model, source, receiver and observed-trace upload */
+    double setup_tune_ms;         /* of setup_ms: autotuning new grid sizes */
 } tti_server_stats;
 
 /* Run-level call: one whole shot from host arrays, synchronously, on a

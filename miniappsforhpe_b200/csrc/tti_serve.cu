@@ -71,7 +71,9 @@ struct tti_server {
     bool stop = false;
     std::map<std::tuple<int, int, int>, GridCost> costs;
     tti_server_stats stats{};
-    std::thread loader, scheduler;
+    std::thread loader, scheduler, retirer;
+    std::deque<std::pair<Shot*, int>> retire;  // finished on the device: read back and free
+    bool scheduler_done = false;
     // scheduler-owned
     cudaStream_t main = nullptr;
     cudaEvent_t fork = nullptr;
@@ -154,11 +156,16 @@ int build_shot(tti_server* srv, Shot* sh)
 {
     const tti_shot_request& r = sh->req;
     tti_sim_config c = shot_config(srv, r, sh->res.checkpoint_every);
+    const double t0 = srv->now();
     int rc = tti_sim_create(&c, &sh->sim);
+    if (!rc) rc = rc_of(cudaStreamSynchronize(shot_stream(sh->sim)));
+    const double t1 = srv->now();
     if (!rc) rc = tti_sim_set_model(sh->sim, r.vp, r.eps, r.delta, r.vs, r.theta, r.phi, r.rho);
     if (!rc) rc = tti_sim_set_source(sh->sim, r.src_ix, r.src_iy, r.src_iz, r.wavelet, r.nt);
     if (!rc) rc = tti_sim_set_receivers(sh->sim, r.nrec, r.rec_ixyz);
     if (!rc) rc = shot_upload_observed(sh->sim, r.observed);
+    if (!rc) rc = rc_of(cudaStreamSynchronize(shot_stream(sh->sim)));
+    const double t2 = srv->now();
     // per-grid cost estimate: autotune on first sight, else a throughput model
     const auto key = std::make_tuple(r.nx, r.ny, r.nz);
     GridCost gc{};
@@ -190,6 +197,13 @@ int build_shot(tti_server* srv, Shot* sh)
         }
     }
     sh->unit_ms = std::max(1e-3, (double)std::max(gc.fwd_ms, gc.adj_ms + gc.img_ms / std::max(1, r.xcorr_step)));
+    {
+        const double t3 = srv->now();
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->stats.setup_alloc_ms += 1e3 * (t1 - t0);
+        srv->stats.setup_model_ms += 1e3 * (t2 - t1);
+        srv->stats.setup_tune_ms += 1e3 * (t3 - t2);
+    }
     if (!rc) rc = shot_begin(sh->sim);
     if (!rc) rc = rc_of(cudaStreamSynchronize(shot_stream(sh->sim)));
     if (!rc) rc = rc_of(cudaEventCreateWithFlags(&sh->join, cudaEventDisableTiming));
@@ -218,6 +232,31 @@ void finish_shot(tti_server* srv, Shot* sh, int status)
     srv->used -= sh->res.footprint;
     srv->resident -= 1;
     srv->done[sh->ticket] = sh;
+    srv->cv.notify_all();
+}
+
+// Read-back and release of finished shots, off the scheduler thread so that
+// the next round is issued while a result is being copied out.
+void retirer_main(tti_server* srv)
+{
+    cudaSetDevice(srv->device);
+    for (;;) {
+        std::pair<Shot*, int> job{nullptr, 0};
+        {
+            std::unique_lock<std::mutex> lk(srv->mu);
+            while (srv->retire.empty() && !srv->scheduler_done) srv->cv.wait_for(lk, std::chrono::milliseconds(50));
+            if (srv->retire.empty()) return;
+            job = srv->retire.front();
+            srv->retire.pop_front();
+        }
+        finish_shot(srv, job.first, job.second);
+    }
+}
+
+void retire_later(tti_server* srv, Shot* sh, int status)
+{
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->retire.push_back({sh, status});
     srv->cv.notify_all();
 }
 
@@ -388,7 +427,7 @@ void scheduler_main(tti_server* srv)
             cudaGetLastError();
             for (Shot* s : inflight_finishing) {
                 active.erase(std::find(active.begin(), active.end(), s));
-                finish_shot(srv, s, shot_end(s->sim));
+                retire_later(srv, s, shot_end(s->sim));
             }
             inflight_finishing.clear();
             inflight = false;
@@ -407,6 +446,7 @@ void scheduler_main(tti_server* srv)
         {
             std::lock_guard<std::mutex> lk(srv->mu);
             srv->stats.rounds++;
+            srv->stats.max_batched = std::max(srv->stats.max_batched, (int)plan.size());
         }
         inflight = true;
         inflight_finishing = finishing;
@@ -436,6 +476,7 @@ int tti_server_create(const tti_server_config* cfg, tti_server** out)
         const int64_t reserve = 2LL << 30;
         srv->cfg.hbm_budget = (int64_t)fr > reserve ? (int64_t)fr - reserve : 0;
     }
+
     // kernel attributes and error words before any capture
     if (!rc) rc = prepare_fused_kernels();
     if (!rc) rc = rc_of(cudaStreamCreateWithFlags(&srv->main, cudaStreamNonBlocking));
@@ -456,6 +497,7 @@ int tti_server_create(const tti_server_config* cfg, tti_server** out)
     }
     srv->loader = std::thread(loader_main, srv);
     srv->scheduler = std::thread(scheduler_main, srv);
+    srv->retirer = std::thread(retirer_main, srv);
     *out = srv;
     return TTI_OK;
 }
@@ -530,6 +572,12 @@ int tti_server_destroy(tti_server* srv)
     }
     srv->loader.join();
     srv->scheduler.join();
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->scheduler_done = true;
+        srv->cv.notify_all();
+    }
+    srv->retirer.join();
     for (auto& kv : srv->done) delete kv.second;
     for (int k = 0; k < 2; ++k)
         if (srv->exec[k]) cudaGraphExecDestroy(srv->exec[k]);

@@ -39,7 +39,8 @@ class ShotResultC(C.Structure):
 
 class ServerStatsC(C.Structure):
     _fields_ = [("rounds", L64), ("graph_updates", L64), ("graph_instantiations", L64),
-                ("max_resident", I), ("busy_ms", D), ("gap_ms", D), ("build_ms", D), ("setup_ms", D)]
+                ("max_resident", I), ("busy_ms", D), ("gap_ms", D), ("build_ms", D), ("setup_ms", D),
+                ("max_batched", I), ("setup_alloc_ms", D), ("setup_model_ms", D), ("setup_tune_ms", D)]
 
 
 _declared = False
@@ -203,7 +204,9 @@ class Server:
             raise TTIError(rc, "tti_server_stats_get")
         return {"rounds": s.rounds, "graph_updates": s.graph_updates,
                 "graph_instantiations": s.graph_instantiations, "max_resident": s.max_resident,
-                "busy_ms": s.busy_ms, "gap_ms": s.gap_ms, "build_ms": s.build_ms, "setup_ms": s.setup_ms}
+                "busy_ms": s.busy_ms, "gap_ms": s.gap_ms, "build_ms": s.build_ms, "setup_ms": s.setup_ms,
+                "max_batched": s.max_batched, "setup_alloc_ms": s.setup_alloc_ms,
+                "setup_model_ms": s.setup_model_ms, "setup_tune_ms": s.setup_tune_ms}
 
     def close(self):
         if self._h:

@@ -15,11 +15,11 @@ from miniappsforhpe_b200 import earth_models as EM
 from miniappsforhpe_b200.serve import Server, Shot
 from tests.helpers import rel_l2
 
-SHOTS = [  # nx, ny, nz, nt, seed
-    (48, 40, 40, 64, 1),
-    (64, 48, 40, 80, 2),
-    (40, 40, 48, 52, 3),
-    (56, 40, 32, 72, 4),
+SHOTS = [  # nx, ny, nz, nt, seed: enough steps that each shot outlasts the set-up of the next
+    (48, 40, 40, 320, 1),
+    (64, 48, 40, 400, 2),
+    (40, 40, 48, 260, 3),
+    (56, 40, 32, 360, 4),
 ]
 
 
@@ -76,6 +76,7 @@ def test_results_are_the_same_alone_and_in_the_mix(shots, reference, graphs):
         st = srv.stats()
     check(res, objs, reference)
     assert st["max_resident"] >= 2  # shots were resident together
+    assert st["max_batched"] >= 2   # and advanced in the same rounds
     assert st["rounds"] > 4         # and advanced over several batched rounds
     assert all(r.units == 2 * s["nt"] for r, s in zip(res, shots))
 
