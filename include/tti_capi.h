@@ -254,6 +254,13 @@ typedef struct {
     int scheme;           /* 0: staggered variable-density operator (kernel_type2, the simulator's
                              own); 1: centred constant-density operator (kernel_type1 launchers;
                              Vp image only, grad_rho stays zero) */
+    int wave_precision;   /* 0: FP32 wavefields.  1 FP16 / 2 BF16 (fused = 1): p and q leave every
+                             step rounded to that format of value * a per-field power-of-two scale
+                             (from the previous step's largest |p|, |q|) and are read back exactly;
+                             stencils, pdot/qdot and the time update stay FP32.  The rounded
+                             values are held in the FP32 arrays (the stencil kernels are
+                             instruction-bound, not byte-bound), so this is the numerics of
+                             FP16/BF16 wavefield storage without its memory saving. */
 } tti_sim_config;
 
 int tti_sim_create(const tti_sim_config* cfg, tti_sim** out);

@@ -57,7 +57,7 @@ class SimConfig(C.Structure):
         ("dx", D), ("dy", D), ("dz", D),
         ("dt", F), ("nt", I), ("xcorr_step", I), ("sponge_width", I),
         ("free_surface", I), ("fused", I), ("save_snapshots", I), ("snap_precision", I),
-        ("checkpoint_every", I), ("use_graphs", I), ("scheme", I),
+        ("checkpoint_every", I), ("use_graphs", I), ("scheme", I), ("wave_precision", I),
     ]
 
 
@@ -323,13 +323,14 @@ class Config:
     checkpoint_every: int = 0  # >0: FP32 checkpoints every K steps, snapshots recomputed per segment
     use_graphs: bool = False  # capture each time loop into a CUDA graph
     scheme: int = 0  # 0: staggered variable-density operator; 1: centred constant-density (type1)
+    wave_precision: str = "fp32"  # p/q rounded each step to "fp16" | "bf16" (per-field scale)
 
     def c_struct(self) -> SimConfig:
         prec = {"fp32": 0, "fp16": 1, "bf16": 2}[self.snap_precision]
         return SimConfig(self.nx, self.ny, self.nz, self.dx, self.dy, self.dz, self.dt, self.nt,
                          self.xcorr_step, self.sponge_width, int(self.free_surface), int(self.fused),
                          int(self.save_snapshots), prec, int(self.checkpoint_every), int(self.use_graphs),
-                         int(self.scheme))
+                         int(self.scheme), {"fp32": 0, "fp16": 1, "bf16": 2}[self.wave_precision])
 
     def footprint_bytes(self) -> int:
         """Device bytes ``tti_sim_create`` allocates for this configuration."""

@@ -76,6 +76,26 @@ __device__ __forceinline__ bool snap_store(void* base, int64_t i, float v, int p
     static_cast<__nv_bfloat16*>(base)[i] = __float2bfloat16_rn(v);
     return false;
 }
+// Reduced-precision wavefields: p and q leave each step rounded to FP16 or
+// BF16 of value*scale and read back exactly (the scale a power of two taken
+// from the largest |p|, |q| of the step before, target 2^11 below the FP16
+// limit; FP16 values beyond its range are clamped, and the maxima pass
+// flags them); the values stay in FP32 arrays.  prec and scale are kernel
+// parameters, so the FP32 path carries no extra registers.
+__device__ __forceinline__ float wave_round(int prec, float v, float s)
+{
+    const float w = v * s;
+    const float r = prec == 1 ? __half2float(__float2half_rn(fminf(fmaxf(w, -65504.0f), 65504.0f)))
+                              : __bfloat162float(__float2bfloat16_rn(w));
+    return r / s;  // a power of two: exact
+}
+__device__ __forceinline__ void wave_apply(int prec, const float* scale, float& p, float& q)
+{
+    if (!prec) return;
+    p = wave_round(prec, p, __ldg(scale));
+    q = wave_round(prec, q, __ldg(scale + 1));
+}
+
 template <typename T> __device__ __forceinline__ float to_f32(T v);
 template <> __device__ __forceinline__ float to_f32<float>(float v) { return v; }
 template <> __device__ __forceinline__ float to_f32<__half>(__half v) { return __half2float(v); }

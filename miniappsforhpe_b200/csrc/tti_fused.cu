@@ -202,6 +202,8 @@ struct FwdParams {
     int fs;
     float dt, invdx, invdy, invdz, invdxdy, invdydz, invdzdx;
     int* err;
+    int wave_prec;            // 0, or p/q rounded to FP16 (1) / BF16 (2) each step
+    const float* wave_scale;  // 2 scales (p, q) of this step's output
 };
 
 constexpr int FWD_NS = 11;  // ring: planes L-8 .. L+2
@@ -506,6 +508,7 @@ __global__ void __launch_bounds__(NT, 1)
                     np = 0.0f;
                     nq = 0.0f;
                 }
+                wave_apply(a.wave_prec, a.wave_scale, np, nq);
                 a.pout[gi] = np;
                 a.qout[gi] = nq;
                 if (a.fs && z > L.izbeg && z <= L.izbeg + kRadius) {
@@ -568,6 +571,8 @@ struct AdjParams {
     int sponge;
     float dt, invdx, invdy, invdz, invdxy, invdyz, invdzx;
     int* err;
+    int wave_prec;            // 0, or p/q rounded to FP16 (1) / BF16 (2) each step
+    const float* wave_scale;  // 2 scales (p, q) of this step's output
 };
 
 // Staging per plane: p, q, m1, m2, m3, m4, irho, rx, ry with a halo of 8 and
@@ -918,6 +923,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
                 np = 0.0f;
                 nq = 0.0f;
             }
+            wave_apply(a.wave_prec, a.wave_scale, np, nq);
             a.pout[gi] = np;
             a.qout[gi] = nq;
             if (a.fs && z > L.izbeg && z <= L.izbeg + kRadius) {
@@ -1336,6 +1342,8 @@ struct T1FwdParams {
     float dt;
     T1Fd k;
     int* err;
+    int wave_prec;            // 0, or p/q rounded to FP16 (1) / BF16 (2) each step
+    const float* wave_scale;  // 2 scales (p, q) of this step's output
 };
 
 // Centred second derivatives of one field at one point, scaled by the
@@ -1556,6 +1564,8 @@ __global__ void __launch_bounds__(T1X2_NT, 2)
                     np = make_float2(0.0f, 0.0f);
                     nq = np;
                 }
+                wave_apply(a.wave_prec, a.wave_scale, np.x, nq.x);
+                if (own_b) wave_apply(a.wave_prec, a.wave_scale, np.y, nq.y);
                 const bool mirror = a.fs && z > L.izbeg && z <= L.izbeg + kRadius;
                 const int64_t gm = L.idx(xa, y, 2 * L.izbeg - z);
                 if (own_b) {
@@ -1648,6 +1658,8 @@ struct T1AdjParams {
     float dt;
     T1Fd k;
     int* err;
+    int wave_prec;            // 0, or p/q rounded to FP16 (1) / BF16 (2) each step
+    const float* wave_scale;  // 2 scales (p, q) of this step's output
 };
 
 template <bool TTI>
@@ -1806,6 +1818,7 @@ __global__ void __launch_bounds__(NT, 1) k_t1_fused_adjoint(const __grid_constan
                     np = 0.0f;
                     nq = 0.0f;
                 }
+                wave_apply(a.wave_prec, a.wave_scale, np, nq);
                 a.pout[go] = np;
                 a.qout[go] = nq;
                 if (a.fs && zo > L.izbeg && zo <= L.izbeg + kRadius) {
@@ -2158,6 +2171,9 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.invdydz = 1.0 / (4 * s.dy * s.dz);
     a.invdzdx = 1.0 / (4 * s.dx * s.dz);
     a.err = s.err ? s.err : err_word();
+    a.wave_prec = s.wave_prec;
+    a.wave_scale = s.wave_scale;
+    if (a.wave_prec && !a.wave_scale) return TTI_EINVAL;
     if (!a.err) return TTI_ENOMEM;
     dim3 grid(cta_count(L, sp));
     if (!kernels_prepared()) return TTI_ELAUNCH;
@@ -2201,6 +2217,9 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     a.invdyz = 1.0 / (4 * s.dy * s.dz);
     a.invdzx = 1.0 / (4 * s.dx * s.dz);
     a.err = s.err ? s.err : err_word();
+    a.wave_prec = s.wave_prec;
+    a.wave_scale = s.wave_scale;
+    if (a.wave_prec && !a.wave_scale) return TTI_EINVAL;
     if (!a.err) return TTI_ENOMEM;
     const bool tti = !s.vti;
     dim3 grid(cta_count(L, sp));
@@ -2349,6 +2368,9 @@ int launch_t1_fused_forward(const Layout& L, const FwdStepArgs& s, int sponge, c
     a.dt = s.dt;
     a.k = t1_fd(s.dx, s.dy, s.dz);
     a.err = s.err ? s.err : err_word();
+    a.wave_prec = s.wave_prec;
+    a.wave_scale = s.wave_scale;
+    if (a.wave_prec && !a.wave_scale) return TTI_EINVAL;
     if (!a.err) return TTI_ENOMEM;
     if (!kernels_prepared()) return TTI_ELAUNCH;
     const dim3 grid(cta_count(L, sp));
@@ -2386,6 +2408,9 @@ int launch_t1_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t 
     a.dt = s.dt;
     a.k = t1_fd(s.dx, s.dy, s.dz);
     a.err = s.err ? s.err : err_word();
+    a.wave_prec = s.wave_prec;
+    a.wave_scale = s.wave_scale;
+    if (a.wave_prec && !a.wave_scale) return TTI_EINVAL;
     if (!a.err) return TTI_ENOMEM;
     if (!kernels_prepared()) return TTI_ELAUNCH;
     const dim3 grid(cta_count(L, sp));

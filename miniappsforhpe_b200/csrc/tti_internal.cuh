@@ -59,6 +59,8 @@ struct FwdStepArgs {
     int* err = nullptr;  // error word of the bounded waits (nullptr: the device's)
     int bz = 0;          // planes per CTA of the tile-major (tile, z) work (0: tuned or modelled)
     int ztop = 0;        // > 0: column tops of ztop planes, bz planes per CTA of the bottoms
+    int wave_prec = 0;                 // p/q leave the step rounded to FP16 (1) or BF16 (2)
+    const float* wave_scale = nullptr; // 2 power-of-two scales (p, q) of the output
 };
 int launch_fused_forward(const Layout& L, const FwdStepArgs& a, cudaStream_t st);
 
@@ -81,6 +83,8 @@ struct AdjStepArgs {
     int* err = nullptr;
     int bz = 0;
     int ztop = 0;
+    int wave_prec = 0;
+    const float* wave_scale = nullptr;
 };
 int launch_fused_adjoint(const Layout& L, const AdjStepArgs& a, cudaStream_t st);
 

@@ -121,10 +121,10 @@ __global__ void k_inject_residual(float* __restrict__ f3, float* __restrict__ f4
 // Per-field power-of-two scale of the next reduced-precision snapshot from
 // the running max |value| of the previous one: max*scale ~ 2^11, leaving a
 // factor 32 of growth before FP16 saturates; the running max is reset.
-__global__ void k_snap_scale(float* __restrict__ scale, unsigned int* __restrict__ amax)
+__global__ void k_snap_scale(float* __restrict__ scale, unsigned int* __restrict__ amax, int nfield)
 {
     const int f = threadIdx.x;
-    if (f >= 4) return;
+    if (f >= nfield) return;
     const float m = __uint_as_float(amax[f]);
     float sc = 1.0f;
     if (m > 0.0f && isfinite(m)) {
@@ -168,6 +168,10 @@ inline int snap_fields(const tti_sim_config& c) { return c.scheme == 1 ? 2 : 4; 
 // second p, q buffer the fused kernels write the next step into.
 struct WaveState {
     float *p = nullptr, *q = nullptr, *pd = nullptr, *qd = nullptr, *p2 = nullptr, *q2 = nullptr;
+    // reduced-precision wavefields: scales (p, q) of the next step's output
+    // and the maxima of |p|, |q| of the current state
+    float* wscale = nullptr;
+    unsigned* wamax = nullptr;
     void swap()
     {
         std::swap(p, p2);
@@ -276,6 +280,7 @@ int validate(const tti_sim_config& c)
         return TTI_EINVAL;
     if (c.snap_precision < 0 || c.snap_precision > 2) return TTI_EINVAL;
     if (c.scheme < 0 || c.scheme > 1) return TTI_EINVAL;
+    if (c.wave_precision < 0 || c.wave_precision > 2 || (c.wave_precision && !c.fused)) return TTI_EINVAL;
     if (c.snap_precision != 0 && (!c.fused || c.nx % 8 != 0)) return TTI_EINVAL;
     if (c.checkpoint_every < 0) return TTI_EINVAL;
     if (c.checkpoint_every > 0 && (c.checkpoint_every % c.xcorr_step != 0 || !c.fused || !c.save_snapshots))
@@ -299,6 +304,8 @@ Plan plan_of(const tti_sim_config& c)
     const size_t nin = (size_t)c.nx * c.ny * c.nz;
     pl.core = 6 * vb + 8 * vb + 2 * nin * sizeof(float) + (size_t)c.nt * sizeof(float) +
               (size_t)(L.ldimx + L.ldimy + L.ldimz) * sizeof(float2) + sizeof(int);
+    const size_t wave = c.wave_precision ? 2 * sizeof(float) + 2 * sizeof(unsigned) : 0;  // scales, maxima
+    pl.core += wave;
     // derivative volumes and scratch: only the staggered scheme's kernel sequence
     pl.need_aux = c.scheme == 0 && (!c.fused || (c.save_snapshots && !fused_image_supported(L)));
     if (pl.need_aux) pl.aux = 10 * vb + 4 * vb;  // rhs3, rhs4, snp, snq, six derivatives, 4-float scratch
@@ -309,7 +316,7 @@ Plan plan_of(const tti_sim_config& c)
             pl.ncp = (c.nt - 1) / c.checkpoint_every + 1;
             pl.nslot = c.checkpoint_every / c.xcorr_step;
             pl.ckpts = (size_t)pl.ncp * 4 * nin * sizeof(float) + (size_t)pl.ncp * 4 * sizeof(unsigned int);
-            pl.recompute = 6 * vb;
+            pl.recompute = 6 * vb + wave;
         }
         pl.snaps = (size_t)pl.nslot * snap_fields(c) * nin * snap_elt_bytes(c.snap_precision) +
                    (size_t)pl.nslot * 4 * sizeof(float) +
@@ -330,7 +337,33 @@ int zero_state(tti_sim* s, WaveState& w, cudaStream_t st = nullptr)
     int rc = TTI_OK;
     for (float* v : {w.p, w.q, w.pd, w.qd, w.p2, w.q2})
         if (!rc && v) rc = sim_zero(s, v, vb, st);
+    if (!rc && w.wamax) rc = sim_zero(s, w.wamax, 2 * sizeof(unsigned), st);
     return rc;
+}
+
+// Largest |p|, |q| of a state's interior (reduced-precision wavefields):
+// the next step's output scales come from it; with FP16, a value at the
+// clamp of the scale it was stored with flags a saturation.
+__global__ void k_wave_amax(const float* __restrict__ p, const float* __restrict__ q, unsigned* amax,
+                            const float* __restrict__ used_scale, int prec, int* err, Layout L)
+{
+    const int64_t n = (int64_t)L.nx() * L.ny() * L.nz();
+    unsigned mp = 0u, mq = 0u;
+    for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < n; d += (int64_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(d % L.nx()), iy = (int)((d / L.nx()) % L.ny()), iz = (int)(d / ((int64_t)L.nx() * L.ny()));
+        const int64_t i = L.idx(ix + L.ixbeg, iy + L.iybeg, iz + L.izbeg);
+        mp = max(mp, __float_as_uint(fabsf(p[i])));
+        mq = max(mq, __float_as_uint(fabsf(q[i])));
+    }
+    mp = __reduce_max_sync(0xffffffffu, mp);
+    mq = __reduce_max_sync(0xffffffffu, mq);
+    if ((threadIdx.x & 31) == 0) {
+        if (mp) atomicMax(amax, mp);
+        if (mq) atomicMax(amax + 1, mq);
+        if (prec == 1 && used_scale &&
+            (__uint_as_float(mp) * used_scale[0] >= 65504.0f || __uint_as_float(mq) * used_scale[1] >= 65504.0f))
+            atomicOr(err, 2);
+    }
 }
 
 // Sponge profile: damping factor G(k) = exp(-(0.3*(W-k)/W)^2) on the k-th cell
@@ -579,9 +612,31 @@ int fused_prologue(tti_sim* s, WaveState& w, cudaStream_t st)
 }
 
 // One fused forward step n on state w; the snapshot (if any) goes to slot k.
+// Reduced-precision wavefields: before a step, the output scales from the
+// maxima of the current state (the maxima are then cleared); after it, the
+// maxima of the new state.
+int wave_scale_step(tti_sim* s, WaveState& w, cudaStream_t st)
+{
+    if (!s->cfg.wave_precision) return TTI_OK;
+    k_snap_scale<<<1, 32, 0, st>>>(w.wscale, w.wamax, 2);
+    s->launches++;
+    return launch_status();
+}
+
+int wave_amax_step(tti_sim* s, WaveState& w, cudaStream_t st)
+{
+    if (!s->cfg.wave_precision) return TTI_OK;
+    const int64_t n = s->ninterior;
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148LL * 8);
+    k_wave_amax<<<blocks, 256, 0, st>>>(w.p, w.q, w.wamax, w.wscale, s->cfg.wave_precision, s->err, s->L);
+    s->launches++;
+    return launch_status();
+}
+
 int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t st)
 {
     const tti_sim_config& c = s->cfg;
+    int rc0 = TTI_OK;
     FwdStepArgs a{};
     a.pin = w.p;
     a.qin = w.q;
@@ -599,7 +654,7 @@ int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t s
     a.snap_prec = c.snap_precision;
     if (slot >= 0 && c.snap_precision != SNAP_F32) {
         float* sc = s->snap_scale + (size_t)slot * 4;
-        k_snap_scale<<<1, 32, 0, st>>>(sc, s->snap_amax);
+        k_snap_scale<<<1, 32, 0, st>>>(sc, s->snap_amax, 4);
         s->launches++;
         a.snap_scale = sc;
         a.snap_amax = s->snap_amax;
@@ -611,6 +666,9 @@ int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t s
     a.dy = c.dy;
     a.dz = c.dz;
     a.err = s->err;
+    if ((rc0 = wave_scale_step(s, w, st))) return rc0;
+    a.wave_prec = c.wave_precision;
+    a.wave_scale = w.wscale;
     mark_begin(s, 0, st);
     int rc = c.scheme == 1 ? launch_t1_fused_forward(s->L, a, s->sponge_active ? 1 : 0, st)
                            : launch_fused_forward(s->L, a, st);
@@ -618,7 +676,7 @@ int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t s
     if (rc) return rc;
     s->launches++;
     w.swap();
-    return TTI_OK;
+    return wave_amax_step(s, w, st);
 }
 
 int fused_adjoint_step(tti_sim* s, cudaStream_t st)
@@ -644,13 +702,17 @@ int fused_adjoint_step(tti_sim* s, cudaStream_t st)
     a.dy = c.dy;
     a.dz = c.dz;
     a.err = s->err;
+    int rc = wave_scale_step(s, w, st);
+    if (rc) return rc;
+    a.wave_prec = c.wave_precision;
+    a.wave_scale = w.wscale;
     mark_begin(s, 1, st);
-    int rc = c.scheme == 1 ? launch_t1_fused_adjoint(s->L, a, st) : launch_fused_adjoint(s->L, a, st);
+    rc = c.scheme == 1 ? launch_t1_fused_adjoint(s->L, a, st) : launch_fused_adjoint(s->L, a, st);
     mark_end(s, st);
     if (rc) return rc;
     s->launches++;
     w.swap();
-    return TTI_OK;
+    return wave_amax_step(s, w, st);
 }
 
 int image_step(tti_sim* s, int slot, cudaStream_t st)
@@ -738,6 +800,13 @@ int restore_checkpoint(tti_sim* s, WaveState& w, int k, cudaStream_t st)
     if (cudaMemcpyAsync(s->snap_amax, s->ckpt_amax + 4 * k, 4 * sizeof(unsigned int), cudaMemcpyDeviceToDevice, st) !=
         cudaSuccess)
         return cuda_rc(cudaGetLastError());
+    // the maxima of the restored state are those the forward pass saw there
+    if (s->cfg.wave_precision) {
+        const int64_t nn = s->ninterior;
+        const int blocks = (int)std::min<int64_t>((nn + 255) / 256, 148LL * 8);
+        k_wave_amax<<<blocks, 256, 0, st>>>(w.p, w.q, w.wamax, nullptr, 0, s->err, s->L);
+        s->launches++;
+    }
     return launch_status();
 }
 
@@ -843,6 +912,10 @@ int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
     for (float** v : {&s->w.p, &s->w.q, &s->w.pd, &s->w.qd, &s->w.p2, &s->w.q2})
         if (!rc) rc = s->alloc((void**)v, vb);
     for (int k = 0; k < 8 && !rc; ++k) rc = s->alloc((void**)&s->mv[k], vb);
+    if (!rc && c.wave_precision) {
+        rc = s->alloc((void**)&s->w.wscale, 2 * sizeof(float));
+        if (!rc) rc = s->alloc((void**)&s->w.wamax, 2 * sizeof(unsigned));
+    }
     if (!rc && pl.need_aux) {
         s->aux = true;
         for (float** v : {&s->rhs3, &s->rhs4, &s->snp, &s->snq, &s->d[0], &s->d[1], &s->d[2], &s->d[3], &s->d[4],
@@ -871,6 +944,10 @@ int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
             if (!rc) rc = s->alloc((void**)&s->ckpt_amax, (size_t)s->ncp * 4 * sizeof(unsigned int));
             for (float** v : {&s->rw.p, &s->rw.q, &s->rw.pd, &s->rw.qd, &s->rw.p2, &s->rw.q2})
                 if (!rc) rc = s->alloc((void**)v, vb);
+            if (!rc && c.wave_precision) {
+                rc = s->alloc((void**)&s->rw.wscale, 2 * sizeof(float));
+                if (!rc) rc = s->alloc((void**)&s->rw.wamax, 2 * sizeof(unsigned));
+            }
         }
     }
     if (!rc) rc = zero_state(s, s->w);

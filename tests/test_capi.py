@@ -149,3 +149,12 @@ def test_work_split_table_round_trip():
     finally:
         for k in P.TUNE_KINDS:
             P.tune_set(64, 48, 40, k, 0)
+
+
+def test_wave_precision_is_validated_and_costs_only_its_scales():
+    base = dict(nx=64, ny=64, nz=64, nt=40, xcorr_step=4, save_snapshots=False)
+    with pytest.raises(P.TTIError) as e:
+        P.Config(**base, fused=False, wave_precision="fp16").footprint_bytes()
+    assert e.value.status == P.EINVAL
+    plain = P.Config(**base).footprint_bytes()
+    assert P.Config(**base, wave_precision="bf16").footprint_bytes() == plain + 16

@@ -62,3 +62,64 @@ def test_reduced_precision_snapshots_against_fp64_oracle():
     assert report["fp32"]["image_vp"] < 1e-5 and report["fp32"]["grad_rho"] < 1e-5
     assert report["fp16"]["image_vp"] < 1e-3 and report["fp16"]["grad_rho"] < 1e-3
     assert report["bf16"]["image_vp"] < 2e-2 and report["bf16"]["grad_rho"] < 2e-2
+
+
+def run_wave(prec, model, nx, ny, nz, nt, dt, w, src, rec, **kw):
+    cfg = P.Config(nx=nx, ny=ny, nz=nz, dt=dt, nt=nt, xcorr_step=4, sponge_width=8, fused=True,
+                   snap_precision=prec, wave_precision=prec, **kw)
+    with P.Simulator(cfg) as sim:
+        sim.set_model(**model)
+        sim.set_source(*src, w)
+        sim.set_receivers(rec)
+        tr = sim.forward()
+        sim.adjoint(tr)
+        gv, gr = sim.image()
+    return tr, gv, gr
+
+
+@pytest.mark.gpu
+def test_reduced_precision_wavefields_against_fp64_oracle():
+    """p and q rounded to FP16 / BF16 (per-field power-of-two scale) at every
+    step, snapshots in the same format, stencils and pdot/qdot in FP32: the
+    error of traces, image and gradient against the FP64 oracle."""
+    nx, ny, nz, nt = 48, 40, 40, 80
+    model = EM.smooth_tti(nx, ny, nz, dx=10.0, corr_m=80.0, seed=21)
+    dt = EM.cfl_dt(model, 10.0)
+    w = EM.ricker(nt, dt, 25.0) * 1e3
+    src = (nx // 2, ny // 2, 5)
+    rec = EM.receiver_plane(nx, ny, 3)
+    cfg, _, _, _, m32 = run("fp32", model, nx, ny, nz, nt, dt, w, src, rec)
+    lay = Layout(nx, ny, nz)
+    m64 = {k: v.astype(np.float64) for k, v in m32.items()}
+    ab = (sponge_profile(nx, lay.ldimx, 8, True), sponge_profile(ny, lay.ldimy, 8, True),
+          sponge_profile(nz, lay.ldimz, 8, False))
+    rec_idx = np.array([lay.index(*r) for r in rec], np.int64)
+    want = oracle_rtm(Oracle("f64"), lay, m64, ab, cfg, lay.index(*src), w.astype(np.float64), rec_idx)
+    report = {}
+    for p in ("fp16", "bf16"):
+        tr, gv, gr = run_wave(p, model, nx, ny, nz, nt, dt, w, src, rec)
+        assert np.all(np.isfinite(tr)) and np.all(np.isfinite(gv))
+        report[p] = {"traces": rel_l2(tr, want["traces"]), "image_vp": rel_l2(gv, want["grad_vp"]),
+                     "grad_rho": rel_l2(gr, want["grad_rho"])}
+    print(json.dumps(report))
+    if os.path.isdir(OUT):
+        with open(os.path.join(OUT, "precision_report_wavefields.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    for k in ("traces", "image_vp", "grad_rho"):
+        assert report["fp16"][k] < 2e-2
+        assert report["bf16"][k] < 2e-1
+
+
+@pytest.mark.gpu
+def test_reduced_precision_wavefields_recompute_exactly():
+    """Checkpointed recomputation restores the per-field scales from the
+    restored state, so the rounded forward field is recomputed bit for bit."""
+    nx, ny, nz, nt = 40, 32, 32, 44
+    model = EM.smooth_tti(nx, ny, nz, dx=10.0, corr_m=80.0, seed=22)
+    dt = EM.cfl_dt(model, 10.0)
+    w = EM.ricker(nt, dt, 25.0) * 1e3
+    args = (model, nx, ny, nz, nt, dt, w, (nx // 2, ny // 2, 5), EM.receiver_plane(nx, ny, 3))
+    plain = run_wave("fp16", *args)
+    ck = run_wave("fp16", *args, checkpoint_every=8)
+    for a, b in zip(ck, plain):
+        np.testing.assert_array_equal(a, b)
