@@ -105,9 +105,9 @@ def test_reduced_precision_wavefields_against_fp64_oracle():
     if os.path.isdir(OUT):
         with open(os.path.join(OUT, "precision_report_wavefields.json"), "w") as f:
             json.dump(report, f, indent=1)
-    for k in ("traces", "image_vp", "grad_rho"):
-        assert report["fp16"][k] < 2e-2
-        assert report["bf16"][k] < 2e-1
+    for k in ("traces", "image_vp", "grad_rho"):  # measured: fp16 <= 2.2e-3, bf16 <= 8.8e-3
+        assert report["fp16"][k] < 5e-3
+        assert report["bf16"][k] < 3e-2
 
 
 @pytest.mark.gpu
