@@ -2042,16 +2042,20 @@ std::vector<int> plane_candidates(const Layout& L)
     return c;
 }
 
-// Modelled time of a step, in plane-iterations of the slowest CTA: one CTA
-// per SM (shared memory bound), each segment pays the 2*LAG-plane pipeline
-// fill, a range of bz planes covers at most ceil((bz-1)/nz)+1 columns (one
-// when whole columns divide evenly).
-double plane_cost(const Layout& L, int bz, int lag)
+// CTAs of a kind resident per SM: shared memory (and registers) allow two
+// of the type1 forward kernel's 256-thread CTAs, one of the others.
+int kind_ctas_per_sm(int kind) { return kind == KIND_T1F ? 2 : 1; }
+
+// Modelled time of a step, in plane-iterations of the slowest CTA: per_sm
+// resident CTAs per SM, each segment pays the 2*LAG-plane pipeline fill, a
+// range of bz planes covers at most ceil((bz-1)/nz)+1 columns (one when
+// whole columns divide evenly).
+double plane_cost(const Layout& L, int bz, int lag, int per_sm)
 {
     const int nz = L.nz();
     const long long ctas = cta_count(L, Split{bz, 0});
-    const int sms = device_sms();
-    const double waves = (double)((ctas + sms - 1) / sms);
+    const long long slots = (long long)device_sms() * per_sm;
+    const double waves = (double)((ctas + slots - 1) / slots);
     int segs;
     if (bz <= nz && nz % bz == 0)
         segs = 1;
@@ -2074,11 +2078,13 @@ bool column_aligned(const Layout& L, int bz) { return bz <= L.nz() && L.nz() % b
 // Modelled cost of a top/bottom split in one wave: the tops (one segment
 // each) against the bottom CTAs, whose bz planes cross at most
 // ceil((bz-1)/span)+1 column bottoms.
-double split_cost(const Layout& L, Split sp, int lag)
+double split_cost(const Layout& L, Split sp, int lag, int per_sm)
 {
     const int span = L.nz() - sp.ztop;
     const int segs = (sp.bz - 1) / span + 2;
-    return std::max(sp.ztop + 2.0 * lag, sp.bz + 2.0 * lag * segs);
+    const long long slots = (long long)device_sms() * per_sm;
+    const double waves = (double)((cta_count(L, sp) + slots - 1) / slots);
+    return waves * std::max(sp.ztop + 2.0 * lag, sp.bz + 2.0 * lag * segs);
 }
 
 int kind_lag(int kind) { return (kind == KIND_T1F || kind == KIND_T1A) ? T1_LAG : LAG; }
@@ -2109,18 +2115,27 @@ std::vector<Split> topbottom_candidates(const Layout& L, int kind)
     return c;
 }
 
-int pick_bz(const Layout& L, int kind)
+// The model's split: the cheapest tile-major candidate (column-aligned only
+// for the kernels that stage many halo'd arrays) or top/bottom split.
+Split pick_split(const Layout& L, int kind)
 {
-    int best = L.nz();
+    Split best{L.nz(), 0};
     double best_cost = 1e300;
     const bool any_split = kind == KIND_FWD || kind == KIND_T1F;  // few staged arrays
-    const int lag = kind_lag(kind);
+    const int lag = kind_lag(kind), per_sm = kind_ctas_per_sm(kind);
     for (int bz : plane_candidates(L)) {
         if (!any_split && !column_aligned(L, bz)) continue;
-        const double cost = plane_cost(L, bz, lag);
+        const double cost = plane_cost(L, bz, lag, per_sm);
         if (cost < best_cost - 1e-9) {
             best_cost = cost;
-            best = bz;
+            best = Split{bz, 0};
+        }
+    }
+    for (const Split& sp : topbottom_candidates(L, kind)) {
+        const double cost = split_cost(L, sp, lag, per_sm);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = sp;
         }
     }
     return best;
@@ -2530,7 +2545,7 @@ Split tuned_split(const Layout& L, int kind)
     return it == g_tuned.end() ? Split{} : it->second;
 }
 
-Split model_split(const Layout& L, int kind) { return Split{pick_bz(L, kind), 0}; }
+Split model_split(const Layout& L, int kind) { return pick_split(L, kind); }
 
 Split choose_split(const Layout& L, int kind)
 {
