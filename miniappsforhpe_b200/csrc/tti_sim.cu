@@ -1681,21 +1681,40 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
     for (int kind = 0; kind < 3 && !rc; ++kind) {
         if (kind == KIND_IMG && !img) continue;
         const int table_kind = !t1 ? kind : (kind == KIND_FWD ? KIND_T1F : KIND_T1A);
-        float best = 1e30f;
-        Split best_sp{};
         const std::vector<Split> cand = split_candidates(L, table_kind);
         const Split modelled = model_split(L, table_kind);
         out->ncand = std::max(out->ncand, (int)cand.size());
-        for (const Split& sp : cand) {
-            if ((rc = launch(kind, sp))) break;  // warm-up
+        auto time_of = [&](const Split& sp, int n, float* ms) -> int {
+            int r = launch(kind, sp);  // warm-up
+            if (r) return r;
             cudaEventRecord(e0, st);
-            for (int r = 0; r < reps && !rc; ++r) rc = launch(kind, sp);
+            for (int k = 0; k < n && !r; ++k) r = launch(kind, sp);
             cudaEventRecord(e1, st);
-            if (rc) break;
-            if ((rc = cuda_rc(cudaEventSynchronize(e1)))) break;
+            if (r) return r;
+            if ((r = cuda_rc(cudaEventSynchronize(e1)))) return r;
+            cudaEventElapsedTime(ms, e0, e1);
+            *ms /= n;
+            return TTI_OK;
+        };
+        // first pass over every candidate, then the three fastest and the
+        // model's choice again with more launches: candidates within a few
+        // per cent of each other are ranked on the longer timing
+        std::vector<std::pair<float, Split>> timed;
+        for (const Split& sp : cand) {
             float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ms /= reps;
+            if ((rc = time_of(sp, reps, &ms))) break;
+            timed.push_back({ms, sp});
+        }
+        if (rc) break;
+        std::sort(timed.begin(), timed.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+        std::vector<Split> finalists;
+        for (size_t k = 0; k < timed.size() && finalists.size() < 3; ++k) finalists.push_back(timed[k].second);
+        if (std::find(finalists.begin(), finalists.end(), modelled) == finalists.end()) finalists.push_back(modelled);
+        float best = 1e30f;
+        Split best_sp{};
+        for (const Split& sp : finalists) {
+            float ms = 0;
+            if ((rc = time_of(sp, 2 * reps + 1, &ms))) break;
             if (sp == modelled) out->model_ms[kind] = ms;
             if (ms < best) {
                 best = ms;
