@@ -458,6 +458,8 @@ typedef struct {
     int use_graphs;      /* 1: one captured graph launch per round */
     int autotune;        /* 1: tune the z-chunk of each new grid size before its first shot */
     int snap_precision;  /* snapshot store of every shot: 0 FP32, 1 FP16, 2 BF16 */
+    int scheme;          /* operator of every shot: 0 staggered variable-density, 1 centred
+                            constant-density (as tti_sim_config.scheme) */
 } tti_server_config;
 
 /* One shot.  Host arrays only; the server reads and writes them while the

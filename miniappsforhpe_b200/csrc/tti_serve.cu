@@ -104,6 +104,7 @@ tti_sim_config shot_config(const tti_server* srv, const tti_shot_request& r, int
     c.fused = 1;
     c.save_snapshots = 1;
     c.snap_precision = srv->cfg.snap_precision;
+    c.scheme = srv->cfg.scheme;
     c.checkpoint_every = ckpt;
     c.use_graphs = 0;
     return c;
@@ -463,7 +464,7 @@ int tti_server_create(const tti_server_config* cfg, tti_server** out)
     if (!cfg || !out) return TTI_EINVAL;
     *out = nullptr;
     if (cfg->max_active < 1 || !(cfg->round_ms > 0) || cfg->hbm_budget < 0 || cfg->snap_precision < 0 ||
-        cfg->snap_precision > 2)
+        cfg->snap_precision > 2 || cfg->scheme < 0 || cfg->scheme > 1)
         return TTI_EINVAL;
     tti_server* srv = new (std::nothrow) tti_server();
     if (!srv) return TTI_ENOMEM;

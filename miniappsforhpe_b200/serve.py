@@ -21,7 +21,7 @@ V, I, F, D, L64 = C.c_void_p, C.c_int, C.c_float, C.c_double, C.c_int64
 
 class ServerConfig(C.Structure):
     _fields_ = [("max_active", I), ("hbm_budget", L64), ("round_ms", F), ("use_graphs", I),
-                ("autotune", I), ("snap_precision", I)]
+                ("autotune", I), ("snap_precision", I), ("scheme", I)]
 
 
 class ShotRequestC(C.Structure):
@@ -167,9 +167,9 @@ class Server:
     """Native shot server; ``submit`` returns a ticket, ``wait`` the result."""
 
     def __init__(self, max_active: int = 8, hbm_budget: int = 0, round_ms: float = 50.0,
-                 use_graphs: bool = True, autotune: bool = True, snap_precision: str = "fp16"):
+                 use_graphs: bool = True, autotune: bool = True, snap_precision: str = "fp16", scheme: int = 0):
         cfg = ServerConfig(max_active, hbm_budget, round_ms, int(use_graphs), int(autotune),
-                           PRECISIONS[snap_precision])
+                           PRECISIONS[snap_precision], int(scheme))
         self._h = V()
         rc = _lib().tti_server_create(C.byref(cfg), C.byref(self._h))
         if rc != OK:

@@ -35,9 +35,9 @@ def make_shot(nx, ny, nz, nt, seed):
                 receivers=rec, observed=obs, sponge_width=6)
 
 
-def alone(s, prec):
+def alone(s, prec, scheme=0):
     cfg = P.Config(nx=s["nx"], ny=s["ny"], nz=s["nz"], dt=s["dt"], nt=s["nt"], xcorr_step=4,
-                   sponge_width=s["sponge_width"], fused=True, snap_precision=prec)
+                   sponge_width=s["sponge_width"], fused=True, snap_precision=prec, scheme=scheme)
     with P.Simulator(cfg) as sim:
         sim.set_model(vp=s["vp"], eps=s["eps"], delta=s["delta"], theta=s["theta"], phi=s["phi"])
         sim.set_source(*s["source"], s["wavelet"])
@@ -56,6 +56,11 @@ def shots():
 @pytest.fixture(scope="module")
 def reference(shots):
     return [alone(s, "fp16") for s in shots]
+
+
+@pytest.fixture(scope="module")
+def reference_type1(shots):
+    return [alone(s, "fp16", scheme=1) for s in shots]
 
 
 def check(res, shots, reference):
@@ -107,3 +112,18 @@ def test_budget_forces_checkpointing_and_serial_admission(shots, reference):
         K = r.checkpoint_every
         if K:  # forward + adjoint + recomputation of every segment but the last
             assert r.units == 2 * s["nt"] + ((s["nt"] - 1) // K) * K
+
+
+@pytest.mark.gpu
+def test_centred_operator_served_in_the_mix(shots, reference_type1):
+    """The same mix with the centred constant-density operator: every result
+    equals the shot run alone (its density image stays zero)."""
+    with Server(max_active=4, round_ms=0.3, use_graphs=True, autotune=False, snap_precision="fp16",
+                scheme=1) as srv:
+        objs = [Shot(**s) for s in shots]
+        tickets = [srv.submit(o) for o in objs]
+        res = [srv.wait(t, 300.0) for t in tickets]
+        st = srv.stats()
+    check(res, objs, reference_type1)
+    assert st["max_batched"] >= 2
+    assert all(not np.any(o.image_rho) for o in objs)
