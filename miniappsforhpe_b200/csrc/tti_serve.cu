@@ -74,6 +74,12 @@ struct tti_server {
     std::thread loader, scheduler, retirer;
     std::deque<std::pair<Shot*, int>> retire;  // finished on the device: read back and free
     bool scheduler_done = false;
+    // The shots' device memory comes from a pool of the server's own that
+    // keeps freed memory mapped, so a new shot reuses a finished one's pages
+    // instead of mapping its stores afresh; when a shot's allocation fails
+    // behind fragmented free chunks the pool is trimmed and the set-up
+    // retried once.
+    cudaMemPool_t pool = nullptr;
     // scheduler-owned
     cudaStream_t main = nullptr;
     cudaEvent_t fork = nullptr;
@@ -153,19 +159,37 @@ int choose_checkpoint(const tti_server* srv, const tti_shot_request& r, int64_t 
     return TTI_OK;
 }
 
-int build_shot(tti_server* srv, Shot* sh)
+// The shot's simulator with its model, source, receivers and observed
+// traces; *t_alloc: when its device memory was in place.
+int setup_sim(tti_server* srv, Shot* sh, double* t_alloc)
 {
     const tti_shot_request& r = sh->req;
     tti_sim_config c = shot_config(srv, r, sh->res.checkpoint_every);
-    const double t0 = srv->now();
-    int rc = tti_sim_create(&c, &sh->sim);
+    int rc = sim_create_in_pool(&c, srv->pool, &sh->sim);
     if (!rc) rc = rc_of(cudaStreamSynchronize(shot_stream(sh->sim)));
-    const double t1 = srv->now();
+    *t_alloc = srv->now();
     if (!rc) rc = tti_sim_set_model(sh->sim, r.vp, r.eps, r.delta, r.vs, r.theta, r.phi, r.rho);
     if (!rc) rc = tti_sim_set_source(sh->sim, r.src_ix, r.src_iy, r.src_iz, r.wavelet, r.nt);
     if (!rc) rc = tti_sim_set_receivers(sh->sim, r.nrec, r.rec_ixyz);
     if (!rc) rc = shot_upload_observed(sh->sim, r.observed);
     if (!rc) rc = rc_of(cudaStreamSynchronize(shot_stream(sh->sim)));
+    return rc;
+}
+
+int build_shot(tti_server* srv, Shot* sh)
+{
+    const tti_shot_request& r = sh->req;
+    double t0 = srv->now(), t1 = t0;
+    int rc = setup_sim(srv, sh, &t1);
+    if (rc == TTI_ENOMEM && srv->pool) {  // free chunks too fragmented: return them and retry once
+        if (sh->sim) {
+            tti_sim_destroy(sh->sim);
+            sh->sim = nullptr;
+        }
+        cudaMemPoolTrimTo(srv->pool, 0);
+        cudaGetLastError();
+        rc = setup_sim(srv, sh, &t1);
+    }
     const double t2 = srv->now();
     // per-grid cost estimate: autotune on first sight, else a throughput model
     const auto key = std::make_tuple(r.nx, r.ny, r.nz);
@@ -478,6 +502,19 @@ int tti_server_create(const tti_server_config* cfg, tti_server** out)
         srv->cfg.hbm_budget = (int64_t)fr > reserve ? (int64_t)fr - reserve : 0;
     }
 
+    if (!rc) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = srv->device;
+        if (cudaMemPoolCreate(&srv->pool, &props) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            srv->pool = nullptr;  // the default pool then
+        }
+        cudaGetLastError();
+    }
     // kernel attributes and error words before any capture
     if (!rc) rc = prepare_fused_kernels();
     if (!rc) rc = rc_of(cudaStreamCreateWithFlags(&srv->main, cudaStreamNonBlocking));
@@ -487,6 +524,7 @@ int tti_server_create(const tti_server_config* cfg, tti_server** out)
         if (!rc) rc = rc_of(cudaEventCreate(&srv->round_end[k]));
     }
     if (rc) {
+        if (srv->pool) cudaMemPoolDestroy(srv->pool);
         if (srv->main) cudaStreamDestroy(srv->main);
         if (srv->fork) cudaEventDestroy(srv->fork);
         for (int k = 0; k < 2; ++k) {
@@ -589,6 +627,7 @@ int tti_server_destroy(tti_server* srv)
         cudaEventDestroy(srv->round_start[k]);
         cudaEventDestroy(srv->round_end[k]);
     }
+    if (srv->pool) cudaMemPoolDestroy(srv->pool);  // every shot's memory has been freed
     cudaGetLastError();
     delete srv;
     return TTI_OK;

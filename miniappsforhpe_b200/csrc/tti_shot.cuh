@@ -9,6 +9,10 @@
 
 namespace tti {
 
+// tti_sim_create with every device allocation of the simulator (and of its
+// model upload) taken from `pool` (nullptr: the device's default pool).
+int sim_create_in_pool(const tti_sim_config* cfg, cudaMemPool_t pool, tti_sim** out);
+
 // Observed traces (nt*nrec, host) for the adjoint's residual; nullptr = zero.
 int shot_upload_observed(tti_sim* s, const float* host_obs);
 // Reset the state and start at forward step 0 (fused, snapshots, model set).

@@ -234,13 +234,18 @@ struct tti_sim {
     // step st_n, last adjoint step st_last, imaged st_imaged)
     int st_mode = 0, st_n = 0, st_last = -1, st_imaged = -1;
 
+    cudaMemPool_t pool = nullptr;  // nullptr: the device's default pool
+    // stream-ordered: creating and destroying simulators never synchronizes
+    // the device
+    cudaError_t raw_alloc(void** p, size_t bytes, cudaStream_t st)
+    {
+        return pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaMallocAsync(p, bytes, st);
+    }
     int alloc(void** p, size_t bytes)
     {
         *p = nullptr;
         if (bytes == 0) return TTI_OK;
-        // stream-ordered: creating and destroying simulators never
-        // synchronizes the device
-        cudaError_t e = cudaMallocAsync(p, bytes, stream);
+        cudaError_t e = raw_alloc(p, bytes, stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             *p = nullptr;
@@ -884,7 +889,11 @@ int tti_sim_footprint_bytes(const tti_sim_config* cfg, int64_t* bytes)
     return TTI_OK;
 }
 
-int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
+int tti_sim_create(const tti_sim_config* cfg, tti_sim** out) { return tti::sim_create_in_pool(cfg, nullptr, out); }
+
+} // extern "C"
+
+int tti::sim_create_in_pool(const tti_sim_config* cfg, cudaMemPool_t pool, tti_sim** out)
 {
     if (!cfg || !out) return TTI_EINVAL;
     *out = nullptr;
@@ -908,6 +917,7 @@ int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
         delete s;
         return TTI_ELAUNCH;
     }
+    s->pool = pool;
     const size_t vb = (size_t)s->nvol() * sizeof(float);
     for (float** v : {&s->w.p, &s->w.q, &s->w.pd, &s->w.qd, &s->w.p2, &s->w.q2})
         if (!rc) rc = s->alloc((void**)v, vb);
@@ -977,6 +987,8 @@ int tti_sim_create(const tti_sim_config* cfg, tti_sim** out)
     return TTI_OK;
 }
 
+extern "C" {
+
 int tti_sim_destroy(tti_sim* s)
 {
     if (!s) return TTI_EINVAL;
@@ -1018,9 +1030,9 @@ int tti_sim_set_model(tti_sim* s, const float* vp, const float* eps, const float
     float* dense = nullptr;
     float* par[7] = {};
     int rc = TTI_OK;
-    if (cudaMallocAsync(&dense, n * sizeof(float), st) != cudaSuccess) return cuda_rc(cudaGetLastError());
+    if (s->raw_alloc((void**)&dense, n * sizeof(float), st) != cudaSuccess) return cuda_rc(cudaGetLastError());
     for (int k = 0; k < 7 && !rc; ++k) {
-        if (cudaMallocAsync(&par[k], s->nvol() * sizeof(float), st) != cudaSuccess) {
+        if (s->raw_alloc((void**)&par[k], s->nvol() * sizeof(float), st) != cudaSuccess) {
             rc = cuda_rc(cudaGetLastError());
             break;
         }
