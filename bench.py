@@ -81,7 +81,9 @@ def parse():
     ap.add_argument("--nt-range", type=int, nargs=2, default=[1000, 3000])
     ap.add_argument("--max-active", type=int, default=8)
     ap.add_argument("--round-ms", type=float, default=50.0)
-    ap.add_argument("--serve-modes", default="served,sequential")
+    ap.add_argument("--serve-modes", default="served,plain",
+                    help="served: the shot server; plain: the run-level call shot by shot in FP32; "
+                         "sequential: the server with one resident shot, FP32")
     return ap.parse_args()
 
 
@@ -554,7 +556,60 @@ def serve_run(args, stream, mode, keep):
     return recs, stats
 
 
+def plain_run(args, stream, keep):
+    """The same stream one shot at a time in plain FP32 through the run-level
+    call (tti_rtm_shot: a simulator created for the shot, fused FP32 kernels,
+    FP32 snapshots, no graphs, no autotuning; checkpoints only for a shot
+    whose snapshots would not fit the free HBM), in arrival order."""
+    import torch
+
+    import miniappsforhpe_b200 as P
+    from miniappsforhpe_b200.serve import rtm_shot
+
+    def options(spec):
+        base = dict(nx=spec["nx"], ny=spec["ny"], nz=spec["nz"], nt=spec["nt"], xcorr_step=4, sponge_width=20)
+        free = torch.cuda.mem_get_info()[0] - (2 << 30)
+        full = P.Config(**base).footprint_bytes()
+        if full <= free:
+            return P.Config(**base), 0
+        best = min(range(4, spec["nt"], 4), key=lambda k: P.Config(**base, checkpoint_every=k).footprint_bytes())
+        return P.Config(**base, checkpoint_every=best), best
+
+    for k, (nx, ny, nz) in enumerate(SERVE_SIZES):  # warm-up, as for the server
+        spec = dict(i=-1, arrival=0.0, nx=nx, ny=ny, nz=nz, nt=16, src=(nx // 2, ny // 2, 2), seed=77 + k)
+        rtm_shot(serve_shot(spec), options(spec)[0])
+    shots = {spec["i"]: serve_shot(spec) for spec in stream}  # built ahead, as the client thread would
+    recs = []
+    busy = 0.0
+    t0 = time.perf_counter()
+    for spec in stream:
+        now = time.perf_counter() - t0
+        if now < spec["arrival"]:
+            time.sleep(spec["arrival"] - now)
+        sh = shots.pop(spec["i"])
+        opts, ck = options(spec)
+        ts = time.perf_counter()
+        rtm_shot(sh, opts)
+        te = time.perf_counter()
+        busy += te - ts
+        rec = dict(i=spec["i"], t_submit=spec["arrival"], t_admit=ts - t0, t_done=te - t0,
+                   latency=te - t0 - spec["arrival"], ckpt=ck, units=0, footprint=opts.footprint_bytes())
+        if spec["i"] in keep:
+            rec["image"] = (sh.image_vp.copy(), sh.image_rho.copy())
+        recs.append(rec)
+    return recs, {"busy_ms": None, "wall_in_calls_s": busy}
+
+
 def serve_summary(recs, stats, stream):
+    if stats.get("busy_ms") is None:  # the plain loop: no server
+        lat = np.array([r["latency"] for r in recs])
+        span = max(r["t_done"] for r in recs) - min(r["t_submit"] for r in recs)
+        pts = sum(s["nx"] * s["ny"] * s["nz"] * s["nt"] for s in stream)
+        return {"shots": len(recs), "shots_per_hour": len(recs) / span * 3600.0, "makespan_s": span,
+                "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                "mean_latency_s": float(lat.mean()), "gpts_per_s": pts / span / 1e9,
+                "checkpointed_shots": int(sum(1 for r in recs if r["ckpt"])),
+                "time_in_shot_calls_s": stats["wall_in_calls_s"]}
     lat = np.array([r["latency"] for r in recs])
     span = max(r["t_done"] for r in recs) - min(r["t_submit"] for r in recs)
     pts = sum(s["nx"] * s["ny"] * s["nz"] * s["nt"] for s in stream)
@@ -575,12 +630,12 @@ def run_serve(args):
     modes = [m for m in args.serve_modes.split(",") if m]
     out, images = {}, {}
     for mode in modes:
-        recs, stats = serve_run(args, stream, mode, keep)
+        recs, stats = plain_run(args, stream, keep) if mode == "plain" else serve_run(args, stream, mode, keep)
         out[mode] = serve_summary(recs, stats, stream)
         images[mode] = {r["i"]: r["image"] for r in recs if "image" in r}
     line = {"metric": METRIC, "mode": "serve", "unit": "shots/hour",
             "value": out.get("served", out.get(modes[0]))["shots_per_hour"], "higher_is_better": True,
-            "n_gpus": 1, "dtype": "f32 stencils, fp16 snapshots (served) / fp32 (sequential)",
+            "n_gpus": 1, "dtype": "f32 stencils, fp16 snapshots (served) / fp32 (plain, sequential)",
             "data": "synthetic (seeded)",
             "config": {"workload": f"served batch: {args.shots} TTI RTM shots, Poisson arrivals {args.rate}/s",
                        "sizes": SERVE_SIZES, "nt_range": args.nt_range, "max_active": args.max_active,
@@ -588,11 +643,14 @@ def run_serve(args):
                        "receivers": "every 4th cell of plane z=3", "sponge_width": 20,
                        "observed": "zero (residual = synthetic traces; work does not depend on the values)"},
             **out}
+    base = "plain" if "plain" in out else "sequential"
     if "served" in out and "sequential" in out:
-        line["speedup_shots_per_hour"] = out["served"]["shots_per_hour"] / out["sequential"]["shots_per_hour"]
+        line["served_vs_server_one_at_a_time"] = out["served"]["shots_per_hour"] / out["sequential"]["shots_per_hour"]
+    if "served" in out and base in out:
+        line["speedup_shots_per_hour"] = out["served"]["shots_per_hour"] / out[base]["shots_per_hour"]
         e = []
         for i, (gv, gr) in images["served"].items():
-            rv, rr = images["sequential"][i]
+            rv, rr = images[base][i]
             e.append((float(np.linalg.norm((gv - rv).astype(np.float64)) / max(np.linalg.norm(rv), 1e-30)),
                       float(np.linalg.norm((gr - rr).astype(np.float64)) / max(np.linalg.norm(rr), 1e-30))))
         line["image_rel_l2_served_vs_fp32"] = {"shots_compared": len(e), "max_vp": max(x[0] for x in e),
