@@ -4,7 +4,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from oracle import DKEYS, MKEYS, Layout, RADIUS
+from oracle import DKEYS, Layout, RADIUS
 
 
 def rel_l2(a, b) -> float:
