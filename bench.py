@@ -350,8 +350,9 @@ def run_ours(args):
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    clk_proc, clk_file = sample_clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")) \
-        if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else sample_clocks(f"/tmp/clocks_rank{rank}.csv")
+    rdir = os.environ.get("TTI_REPORT_DIR")  # where the clock samples are kept, if set
+    clk_proc, clk_file = sample_clocks(os.path.join(rdir if rdir and os.path.isdir(rdir) else "/tmp",
+                                                    f"clocks_rank{rank}.csv"))
     sim.set_profiling(True)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)

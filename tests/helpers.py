@@ -2,9 +2,17 @@
 comparison metrics."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 from oracle import DKEYS, Layout, RADIUS
+
+
+def report_dir():
+    """Directory for JSON reports of the GPU tests (TTI_REPORT_DIR), or None."""
+    d = os.environ.get("TTI_REPORT_DIR")
+    return d if d and os.path.isdir(d) else None
 
 
 def rel_l2(a, b) -> float:

@@ -13,9 +13,8 @@ import pytest
 import miniappsforhpe_b200 as P
 from miniappsforhpe_b200 import earth_models as EM
 from oracle import Layout, Oracle
-from tests.helpers import oracle_rtm, rel_l2, sim_models, sponge_profile
+from tests.helpers import oracle_rtm, rel_l2, report_dir, sim_models, sponge_profile
 
-OUT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpurun_out")
 
 
 def run(prec, model, nx, ny, nz, nt, dt, w, src, rec):
@@ -53,8 +52,8 @@ def test_reduced_precision_snapshots_against_fp64_oracle():
         report[p] = {"traces": rel_l2(tr, want["traces"]), "image_vp": rel_l2(gv, want["grad_vp"]),
                      "grad_rho": rel_l2(gr, want["grad_rho"])}
     print(json.dumps(report))
-    if os.path.isdir(OUT):
-        with open(os.path.join(OUT, "precision_report.json"), "w") as f:
+    if report_dir():
+        with open(os.path.join(report_dir(), "precision_report.json"), "w") as f:
             json.dump(report, f, indent=1)
     np.testing.assert_array_equal(res["fp16"][1], res["fp32"][1])
     np.testing.assert_array_equal(res["bf16"][1], res["fp32"][1])
@@ -102,8 +101,8 @@ def test_reduced_precision_wavefields_against_fp64_oracle():
         report[p] = {"traces": rel_l2(tr, want["traces"]), "image_vp": rel_l2(gv, want["grad_vp"]),
                      "grad_rho": rel_l2(gr, want["grad_rho"])}
     print(json.dumps(report))
-    if os.path.isdir(OUT):
-        with open(os.path.join(OUT, "precision_report_wavefields.json"), "w") as f:
+    if report_dir():
+        with open(os.path.join(report_dir(), "precision_report_wavefields.json"), "w") as f:
             json.dump(report, f, indent=1)
     for k in ("traces", "image_vp", "grad_rho"):  # measured: fp16 <= 2.2e-3, bf16 <= 8.8e-3
         assert report["fp16"][k] < 5e-3
