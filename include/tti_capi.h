@@ -512,7 +512,8 @@ typedef struct {
  * driven by observed - synthetic traces, or by the synthetic traces when
  * observed is NULL, images into image_vp / image_rho).  opts (NULL =
  * defaults) contributes only fused, snap_precision, checkpoint_every,
- * use_graphs and scheme; the physical set-up comes from the request. */
+ * use_graphs, scheme and wave_precision; the physical set-up comes from
+ * the request. */
 int tti_rtm_shot(const tti_shot_request* req, const tti_sim_config* opts);
 
 int tti_server_create(const tti_server_config* cfg, tti_server** out);

@@ -1399,6 +1399,7 @@ int tti_rtm_shot(const tti_shot_request* r, const tti_sim_config* opts)
     c.checkpoint_every = opts ? opts->checkpoint_every : 0;
     c.use_graphs = opts ? opts->use_graphs : 0;
     c.scheme = opts ? opts->scheme : 0;
+    c.wave_precision = opts ? opts->wave_precision : 0;
     tti_sim* s = nullptr;
     int rc = tti_sim_create(&c, &s);
     if (!rc) rc = tti_sim_set_model(s, r->vp, r->eps, r->delta, r->vs, r->theta, r->phi, r->rho);

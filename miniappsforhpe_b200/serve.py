@@ -154,7 +154,8 @@ def rtm_shot(shot: Shot, opts=None) -> Shot:
     """One whole shot, synchronously (tti_rtm_shot): fills ``shot.image_vp``,
     ``shot.image_rho`` and ``shot.traces``.  ``opts`` is a
     ``miniappsforhpe_b200.Config`` whose fused, snap_precision,
-    checkpoint_every, use_graphs and scheme fields are used (None: defaults)."""
+    checkpoint_every, use_graphs, scheme and wave_precision fields are used
+    (None: defaults)."""
     req = shot._c()
     cfg = opts.c_struct() if opts is not None else None
     rc = _lib().tti_rtm_shot(C.byref(req), C.byref(cfg) if cfg is not None else None)
