@@ -158,3 +158,57 @@ def test_wave_precision_is_validated_and_costs_only_its_scales():
     assert e.value.status == P.EINVAL
     plain = P.Config(**base).footprint_bytes()
     assert P.Config(**base, wave_precision="bf16").footprint_bytes() == plain + 16
+
+
+def _vp(n):
+    return [C.c_void_p(1)] * n  # never dereferenced: the checks come first
+
+
+def test_type1_launchers_reject_bad_arguments():
+    """Order, ranges, missing volumes and the sponge/calc_snap combination are
+    refused before anything reaches the device (the reference aborts)."""
+    lib = P.lib()
+    fwd, adj = lib.tti_launch_type1_fwd, lib.tti_launch_type1_adj
+    fwd.restype = adj.restype = C.c_int
+    dims = [4, 27, 4, 23, 4, 19, 32, 28, 24]  # ranges, ldimx/y/z
+    tail = [C.c_float(1e-3), C.c_double(10.0), C.c_double(10.0), C.c_double(10.0)]
+    ok_fwd = _vp(14) + dims + [32, 28, 24] + tail
+    assert fwd(*ok_fwd, 16, None, 0, 0, 0) == P.EINVAL                       # order
+    assert fwd(*ok_fwd, 8, None, 1, 1, 0) == P.EINVAL                        # calc_snap with the sponge
+    assert fwd(*(_vp(14) + [4, 27, 4, 23, 4, 19, 28, 28, 24] + [32, 28, 24] + tail), 8, None, 0, 0, 0) == P.EINVAL
+    assert fwd(*([None] + _vp(13) + dims + [32, 28, 24] + tail), 8, None, 0, 0, 0) == P.EINVAL
+    assert fwd(*(_vp(11) + [None] * 3 + dims + [32, 28, 24] + tail), 8, None, 0, 1, 0) == P.EINVAL
+    ok_adj = _vp(14) + dims + tail
+    assert adj(*ok_adj, 12, None, 0, 0) == P.EINVAL
+    assert adj(*(_vp(4) + [None] + _vp(9) + dims + tail), 8, None, 0, 0) == P.EINVAL
+
+
+def test_noalloc_launcher_rejects_a_range_beyond_its_array():
+    lib = P.lib()
+    f = lib.tti_launch_adj_kernel2_drv_noalloc
+    f.restype = C.c_int
+    one = C.c_float(1.0)
+    # 120 x 120 x 80 interior: 160 * 128 * 88 cells > 2^20
+    args = _vp(18) + [4, 123, 4, 123, 4, 83] + [one] * 6 + [160, 128, 8] + [one] * 4 + [None]
+    assert f(*args) == P.ETOOBIG
+    args = _vp(18) + [4, 123, 4, 123, 4, 83] + [one] * 6 + [160, 128, 6] + [one] * 4 + [None]
+    assert f(*args) == P.EINVAL  # order checked first
+
+
+def test_step_and_run_level_calls_reject_missing_objects():
+    lib = P.lib()
+    for name, extra in (("tti_sim_forward_begin", []), ("tti_sim_forward_step", [0]),
+                        ("tti_sim_adjoint_step", [0]), ("tti_sim_image_step", [0]),
+                        ("tti_sim_adjoint_finish", []), ("tti_sim_sync", [])):
+        assert getattr(lib, name)(None, *extra) == P.EINVAL, name
+    lib.tti_rtm_shot.restype = C.c_int
+    assert lib.tti_rtm_shot(None, None) == P.EINVAL
+
+
+def test_server_config_is_validated():
+    from miniappsforhpe_b200 import serve as S
+
+    for kw in (dict(max_active=0), dict(round_ms=0.0), dict(scheme=2)):
+        with pytest.raises(P.TTIError) as e:
+            S.Server(**kw)
+        assert e.value.status == P.EINVAL
