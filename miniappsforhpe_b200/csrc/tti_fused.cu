@@ -21,6 +21,14 @@
 // is preserved and the free-surface mirror can be resolved at output time.
 // Output for plane z happens when plane z+7 arrives.
 //
+// The grid's (tile, z) planes are split among CTAs either tile-major (bz
+// consecutive planes each) or, on grids with fewer tile columns than SMs,
+// top/bottom (a CTA per column top, the others sharing the bottoms); the
+// split changes the launch shape only.  The centred (type1) operator has its
+// own step kernels here as well (output lag 4; the forward one computes two
+// x-neighbouring outputs per thread), and every step kernel can round the
+// p, q it writes to FP16/BF16 of a per-field scaled value.
+//
 // Every mbarrier wait is bounded (clock-based); a wait that gives up sets the
 // error word the host reads back, and the kernel stops waiting.
 
