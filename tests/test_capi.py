@@ -212,3 +212,19 @@ def test_server_config_is_validated():
         with pytest.raises(P.TTIError) as e:
             S.Server(**kw)
         assert e.value.status == P.EINVAL
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/tti_capi.h compiles as C99 on its own (the drop-in boundary is
+    a C header, not a C++ one)."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    src = tmp_path / "use.c"
+    src.write_text('#include "tti_capi.h"\nint main(void) { tti_sim_config c = {0}; (void)c; return 0; }\n')
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-pedantic", "-fsyntax-only",
+                        "-I" + os.path.dirname(HEADER), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
