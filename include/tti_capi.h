@@ -85,7 +85,12 @@ int tti_launch_update_rho_fwd_main_loop_2_1(
 /* Adjoint derivatives and mixed-derivative rhs.  Replaces
  * adj_kernel3_derivatives::launch_adj_kernel2_drv
  * (kernels/kernel_type2_grad_snap.h:7-12).  Model volumes must be finite
- * and Model11 non-zero in the x/y/z halo (the temporaries are formed there). */
+ * and Model11 non-zero in the x/y/z halo (the temporaries are formed there).
+ * Like the reference launcher it keeps no state: its scratch (16 bytes per
+ * cell up to plane izend+4) is allocated and freed in stream order on
+ * `stream` (cudaMallocAsync / cudaFreeAsync), so calls on different streams
+ * never share memory and no call synchronizes the device; TTI_ENOMEM when
+ * the allocation fails. */
 int tti_launch_adj_kernel2_drv(float* dfield1dx, float* dfield2dx, float* dfield1dy, float* dfield2dy,
                                float* dfield1dz, float* dfield2dz, float* field3_rhs, float* field4_rhs,
                                const float* field1, const float* field2, const float* Model11, const float* model1,
@@ -98,13 +103,15 @@ int tti_launch_adj_kernel2_drv(float* dfield1dx, float* dfield2dx, float* dfield
 /* Same computation and arguments as tti_launch_adj_kernel2_drv, with a
  * scratch that is never allocated: no counterpart in the reference.  For
  * callers that must not have the library allocate device memory (their own
- * pool holds HBM, or they cannot take the device-wide synchronize of a
- * growing scratch).  The scratch is a fixed array of
+ * pool holds HBM, their device pool is configured for their own use, or
+ * they must know the footprint up front).  The scratch is a fixed array of
  * TTI_NOALLOC_SCRATCH_CELLS cells (16 MiB); a request with
  * ldimx * ldimy * (izend + 5) above that returns TTI_ETOOBIG.  The first
  * call on a device looks up the array's address and should come before any
- * stream capture.  All calls on a device share the array: calls that overlap
- * on the GPU race and must be ordered by the caller. */
+ * stream capture; the address is kept for the process, so the entry point
+ * does not survive cudaDeviceReset (or any new primary context) on that
+ * device.  All calls on a device share the array: calls that overlap on the
+ * GPU race and must be ordered by the caller. */
 #define TTI_NOALLOC_SCRATCH_CELLS (1 << 20)
 int tti_launch_adj_kernel2_drv_noalloc(float* dfield1dx, float* dfield2dx, float* dfield1dy, float* dfield2dy,
                                        float* dfield1dz, float* dfield2dz, float* field3_rhs, float* field4_rhs,
@@ -131,7 +138,8 @@ int tti_launch_update_adj_kernel_main_3(float* field3, float* field4, const floa
 /* Density gradient grad -= irho*sum(adj*D+fwd + D-adj*fwd).  Replaces
  * launch_update_rho_gradient_rho (kernels/kernel_type2_grad.h:22-32).
  * grad is not offset (element 0 is the first interior point) and has its
- * own leading dimensions, as in the reference. */
+ * own leading dimensions, as in the reference.  Its scratch is taken and
+ * returned in stream order on `stream`, as in tti_launch_adj_kernel2_drv. */
 int tti_launch_update_rho_gradient_rho(float* grad, const float* fwd_field1_dx, const float* fwd_field2_dx,
                                        const float* fwd_field1_dy, const float* fwd_field2_dy,
                                        const float* fwd_field1_dz, const float* fwd_field2_dz, const float* field1,
@@ -209,8 +217,9 @@ int tti_launch_type1_fwd(float* field3, float* field4, const float* field1, cons
                          int use_sponge, int simple);
 
 /* Replaces adj_main_loop_2_inner_gpu::launch (kernels/kernel_type1_gpu_adj.h:6-9):
- * field3/4 += dt * D(M^T (field1, field2)) (or the sponge form).  Uses the
- * library's four-float scratch over the halo'd range. */
+ * field3/4 += dt * D(M^T (field1, field2)) (or the sponge form).  Its
+ * four-float scratch over the halo'd range is taken and returned in stream
+ * order on `stream`, as in tti_launch_adj_kernel2_drv. */
 int tti_launch_type1_adj(float* field3, float* field4, const float* field1, const float* field2, const float* model1,
                          const float* model2, const float* model3, const float* model4, const float* model5,
                          const float* model6, const float* model7, const float* ABx, const float* ABy,

@@ -355,6 +355,13 @@ def _host_f32(a, n):
     return a
 
 
+def _host_out(a, n):
+    """A caller's host output array: float32, C-contiguous, n values."""
+    if not isinstance(a, np.ndarray) or a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"] or a.size != n:
+        raise ValueError(f"host output must be a C-contiguous float32 numpy array of {n} values")
+    return a
+
+
 class Simulator:
     """The ``simulator2SetUp`` call surface on one B200 (include/tti_capi.h section 2)."""
 
@@ -411,11 +418,13 @@ class Simulator:
 
     def forward(self, traces_out=None):
         """Forward loop; returns the (nt, nrec) pressure traces as numpy, or
-        writes them into a CUDA tensor given as ``traces_out``."""
-        if traces_out is not None:
+        writes them into ``traces_out``: a CUDA tensor, or a C-contiguous
+        float32 numpy array of nt*nrec values (host memory, pinned or not)."""
+        if traces_out is not None and hasattr(traces_out, "data_ptr"):
             self._chk(lib().tti_sim_forward(self._h, _ptr(traces_out), 1), "tti_sim_forward")
             return traces_out
-        out = np.zeros((self.cfg.nt, self.nrec), np.float32)
+        out = np.zeros((self.cfg.nt, self.nrec), np.float32) if traces_out is None else _host_out(
+            traces_out, self.cfg.nt * self.nrec)
         p = out.ctypes.data_as(V) if self.nrec else None
         self._chk(lib().tti_sim_forward(self._h, p, 0), "tti_sim_forward")
         return out
@@ -488,14 +497,16 @@ class Simulator:
                 for i, k in enumerate(kinds) if r.bz[i] > 0} | {"candidates": r.ncand}
 
     def image(self, out_vp=None, out_rho=None):
-        """(grad_vp, grad_rho), each (nz, ny, nx); CUDA tensors if given."""
-        if out_vp is not None:
+        """(grad_vp, grad_rho), each (nz, ny, nx): new numpy arrays, or the
+        given outputs (CUDA tensors, or C-contiguous float32 numpy arrays)."""
+        if out_vp is not None and hasattr(out_vp, "data_ptr"):
             self._chk(lib().tti_sim_get_image(self._h, _ptr(out_vp), _ptr(out_rho), 1),
                       "tti_sim_get_image")
             return out_vp, out_rho
         c = self.cfg
-        gv = np.zeros((c.nz, c.ny, c.nx), np.float32)
-        gr = np.zeros((c.nz, c.ny, c.nx), np.float32)
+        n = c.nx * c.ny * c.nz
+        gv = np.zeros((c.nz, c.ny, c.nx), np.float32) if out_vp is None else _host_out(out_vp, n)
+        gr = np.zeros((c.nz, c.ny, c.nx), np.float32) if out_rho is None else _host_out(out_rho, n)
         self._chk(lib().tti_sim_get_image(self._h, gv.ctypes.data_as(V), gr.ctypes.data_as(V), 0),
                   "tti_sim_get_image")
         return gv, gr

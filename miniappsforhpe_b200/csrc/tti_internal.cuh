@@ -10,9 +10,32 @@
 
 namespace tti {
 
-// Per-device scratch of nelem float4 cells owned by the library (grown on
-// demand, kept for the process lifetime); nullptr if it cannot be allocated.
-float4* library_scratch(size_t nelem);
+// Scratch of nelem float4 cells for one launcher call, allocated and freed
+// in stream order on that call's stream (cudaMallocAsync / cudaFreeAsync):
+// nothing is kept between calls, calls on different streams never share
+// memory, and no call synchronizes the device.  get() is nullptr when the
+// allocation failed.
+class CallScratch {
+public:
+    CallScratch(size_t nelem, cudaStream_t st) : st_(st)
+    {
+        if (cudaMallocAsync(reinterpret_cast<void**>(&p_), nelem * sizeof(float4), st) != cudaSuccess) {
+            cudaGetLastError();
+            p_ = nullptr;
+        }
+    }
+    ~CallScratch()
+    {
+        if (p_) cudaFreeAsync(p_, st_);
+    }
+    CallScratch(const CallScratch&) = delete;
+    CallScratch& operator=(const CallScratch&) = delete;
+    float4* get() const { return p_; }
+
+private:
+    float4* p_ = nullptr;
+    cudaStream_t st_;
+};
 
 int launch_base(const float* f1, const float* f2, const float* m1, const float* m2, const float* m3,
                 const float* m4, float4* base, int ixbeg, int ixend, int iybeg, int iyend, int izbeg, int izend,

@@ -1,15 +1,14 @@
 // Adjoint derivatives with a fixed, statically allocated scratch volume.
 //
-// tti_launch_adj_kernel2_drv keeps its four-float-per-cell scratch (the
-// point-wise transposed model) in memory the library cudaMallocs on the first
-// call and re-allocates, after a cudaDeviceSynchronize and a cudaFree, when a
-// later call needs more.  Some callers cannot let a library allocate:
+// tti_launch_adj_kernel2_drv takes its four-float-per-cell scratch (the
+// point-wise transposed model) from the device's stream-ordered allocator on
+// every call.  Some callers cannot let a library allocate:
 //   * a host framework that owns the device memory through its own pool and
-//     has reserved most of HBM for it, so a cudaMalloc behind its back fails
+//     has reserved most of HBM for it, so an allocation behind its back fails
 //     or pushes the pool out of memory;
-//   * a caller that keeps several streams busy (wavefield steps, snapshot
-//     copies) and cannot accept the device-wide stall of the synchronize and
-//     cudaFree done when the scratch grows;
+//   * a caller whose device memory pool is configured for its own use (a
+//     release threshold, access flags, a pool it does not want the library's
+//     blocks mixed into);
 //   * a caller that must know its full device footprint up front, before the
 //     first step runs.
 // tti_launch_adj_kernel2_drv_noalloc serves them: its scratch is a

@@ -30,18 +30,40 @@ using namespace tti;
 
 namespace {
 
-// Interior (nx*ny*nz, x fastest) -> halo'd volume, halo by edge extension.
-__global__ void k_scatter_extend(float* __restrict__ vol, const float* __restrict__ in, Layout L)
+// Model set-up in one pass over the halo'd volumes: every cell takes the
+// parameters of the nearest interior cell (edge extension on every axis,
+// the x padding included), applies init_cijs (simulator2SetUp.cu:10-29) and
+// writes the buoyancy irho = 1/rho (IEEE division; the reference never sets
+// Model11, kernel_type2.cu:136-141).  par holds the dense interior arrays
+// vp, eps, delta, vs, theta, phi, rho; a null entry takes its default (0,
+// rho 1).  Any theta != 0 marks the model TTI in *tti_flag.
+struct ModelOut {
+    float* v[8];  // irho, model1..model4, rx, ry, rz
+};
+struct ModelIn {
+    const float* p[7];
+};
+__global__ void k_model_setup(ModelOut out, ModelIn par, Layout L, int* __restrict__ tti_flag)
 {
-    int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    int iy = blockIdx.y;
-    int iz = blockIdx.z;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;  // ldimx is a multiple of 32: whole warps leave
+    const int iy = blockIdx.y, iz = blockIdx.z;
     if (ix >= L.ldimx) return;
-    int nx = L.nx(), ny = L.ny(), nz = L.nz();
-    int jx = min(max(ix - L.ixbeg, 0), nx - 1);
-    int jy = min(max(iy - L.iybeg, 0), ny - 1);
-    int jz = min(max(iz - L.izbeg, 0), nz - 1);
-    vol[L.idx(ix, iy, iz)] = in[((int64_t)jz * ny + jy) * nx + jx];
+    const int nx = L.nx(), ny = L.ny(), nz = L.nz();
+    const int jx = min(max(ix - L.ixbeg, 0), nx - 1);
+    const int jy = min(max(iy - L.iybeg, 0), ny - 1);
+    const int jz = min(max(iz - L.izbeg, 0), nz - 1);
+    const int64_t d = ((int64_t)jz * ny + jy) * nx + jx;
+    const float dflt[7] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f};
+    float v[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) v[k] = par.p[k] ? __ldg(par.p[k] + d) : dflt[k];
+    const int64_t g = L.idx(ix, iy, iz);
+    float m[7];
+    init_cij_cell(v[0], v[1], v[2], v[3], v[4], v[5], m[0], m[1], m[2], m[3], m[4], m[5], m[6]);
+    out.v[0][g] = 1.0f / v[6];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) out.v[k + 1][g] = m[k];
+    if (__any_sync(0xffffffffu, v[4] != 0.0f) && (threadIdx.x & 31) == 0) atomicOr(tti_flag, 1);
 }
 
 // Interior copy between a halo'd volume and a dense interior array.
@@ -346,27 +368,38 @@ int zero_state(tti_sim* s, WaveState& w, cudaStream_t st = nullptr)
     return rc;
 }
 
-// Largest |p|, |q| of a state's interior (reduced-precision wavefields):
-// the next step's output scales come from it; with FP16, a value at the
-// clamp of the scale it was stored with flags a saturation.
-__global__ void k_wave_amax(const float* __restrict__ p, const float* __restrict__ q, unsigned* amax,
+// Reduced-precision wavefields: the size of the p, q the next step will
+// write, estimated from the state it starts from (run just before the step,
+// after any injection into pdot, qdot): max over the interior of
+// |p| + dt*|pdot| (and the same for q), since the step writes about
+// A*p + B*dt*pdot.  The output scales come from it, so a wavefield that
+// starts from rest gets a scale from its first non-zero pdot instead of
+// having its first small values flushed to zero.  With FP16, a stored p or q
+// at the clamp of the scale it was stored with flags a saturation.
+__global__ void k_wave_amax(const float* __restrict__ p, const float* __restrict__ q, const float* __restrict__ pd,
+                            const float* __restrict__ qd, float dt, unsigned* amax,
                             const float* __restrict__ used_scale, int prec, int* err, Layout L)
 {
     const int64_t n = (int64_t)L.nx() * L.ny() * L.nz();
-    unsigned mp = 0u, mq = 0u;
+    unsigned mp = 0u, mq = 0u;    // bits of max |p| + dt|pdot| (non-negative floats order like their bits)
+    float sp = 0.0f, sq = 0.0f;   // max |p|, |q| as stored
     for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < n; d += (int64_t)gridDim.x * blockDim.x) {
         const int ix = (int)(d % L.nx()), iy = (int)((d / L.nx()) % L.ny()), iz = (int)(d / ((int64_t)L.nx() * L.ny()));
         const int64_t i = L.idx(ix + L.ixbeg, iy + L.iybeg, iz + L.izbeg);
-        mp = max(mp, __float_as_uint(fabsf(p[i])));
-        mq = max(mq, __float_as_uint(fabsf(q[i])));
+        const float ap = fabsf(p[i]), aq = fabsf(q[i]);
+        sp = fmaxf(sp, ap);
+        sq = fmaxf(sq, aq);
+        mp = max(mp, __float_as_uint(ap + dt * fabsf(pd[i])));
+        mq = max(mq, __float_as_uint(aq + dt * fabsf(qd[i])));
     }
     mp = __reduce_max_sync(0xffffffffu, mp);
     mq = __reduce_max_sync(0xffffffffu, mq);
+    sp = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(sp)));
+    sq = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(sq)));
     if ((threadIdx.x & 31) == 0) {
         if (mp) atomicMax(amax, mp);
         if (mq) atomicMax(amax + 1, mq);
-        if (prec == 1 && used_scale &&
-            (__uint_as_float(mp) * used_scale[0] >= 65504.0f || __uint_as_float(mq) * used_scale[1] >= 65504.0f))
+        if (prec == 1 && used_scale && (sp * used_scale[0] >= 65504.0f || sq * used_scale[1] >= 65504.0f))
             atomicOr(err, 2);
     }
 }
@@ -617,24 +650,20 @@ int fused_prologue(tti_sim* s, WaveState& w, cudaStream_t st)
 }
 
 // One fused forward step n on state w; the snapshot (if any) goes to slot k.
-// Reduced-precision wavefields: before a step, the output scales from the
-// maxima of the current state (the maxima are then cleared); after it, the
-// maxima of the new state.
+// Reduced-precision wavefields: just before a step, the estimated size of
+// its output from the state it starts from, then the output scales from it
+// (the maxima are cleared again).  The scales are a function of the state
+// alone, so a forward step recomputed from a checkpoint rounds exactly as
+// the first time.
 int wave_scale_step(tti_sim* s, WaveState& w, cudaStream_t st)
-{
-    if (!s->cfg.wave_precision) return TTI_OK;
-    k_snap_scale<<<1, 32, 0, st>>>(w.wscale, w.wamax, 2);
-    s->launches++;
-    return launch_status();
-}
-
-int wave_amax_step(tti_sim* s, WaveState& w, cudaStream_t st)
 {
     if (!s->cfg.wave_precision) return TTI_OK;
     const int64_t n = s->ninterior;
     const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148LL * 8);
-    k_wave_amax<<<blocks, 256, 0, st>>>(w.p, w.q, w.wamax, w.wscale, s->cfg.wave_precision, s->err, s->L);
-    s->launches++;
+    k_wave_amax<<<blocks, 256, 0, st>>>(w.p, w.q, w.pd, w.qd, s->cfg.dt, w.wamax, w.wscale, s->cfg.wave_precision,
+                                        s->err, s->L);
+    k_snap_scale<<<1, 32, 0, st>>>(w.wscale, w.wamax, 2);
+    s->launches += 2;
     return launch_status();
 }
 
@@ -681,7 +710,7 @@ int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t s
     if (rc) return rc;
     s->launches++;
     w.swap();
-    return wave_amax_step(s, w, st);
+    return TTI_OK;
 }
 
 int fused_adjoint_step(tti_sim* s, cudaStream_t st)
@@ -717,7 +746,7 @@ int fused_adjoint_step(tti_sim* s, cudaStream_t st)
     if (rc) return rc;
     s->launches++;
     w.swap();
-    return wave_amax_step(s, w, st);
+    return TTI_OK;
 }
 
 int image_step(tti_sim* s, int slot, cudaStream_t st)
@@ -805,13 +834,6 @@ int restore_checkpoint(tti_sim* s, WaveState& w, int k, cudaStream_t st)
     if (cudaMemcpyAsync(s->snap_amax, s->ckpt_amax + 4 * k, 4 * sizeof(unsigned int), cudaMemcpyDeviceToDevice, st) !=
         cudaSuccess)
         return cuda_rc(cudaGetLastError());
-    // the maxima of the restored state are those the forward pass saw there
-    if (s->cfg.wave_precision) {
-        const int64_t nn = s->ninterior;
-        const int blocks = (int)std::min<int64_t>((nn + 255) / 256, 148LL * 8);
-        k_wave_amax<<<blocks, 256, 0, st>>>(w.p, w.q, w.wamax, nullptr, 0, s->err, s->L);
-        s->launches++;
-    }
     return launch_status();
 }
 
@@ -1014,58 +1036,43 @@ int tti_sim_set_model(tti_sim* s, const float* vp, const float* eps, const float
     const int64_t n = s->ninterior;
     const Layout& L = s->L;
     cudaStream_t st = s->stream;
-    // Six host parameter arrays (plus rho) uploaded as interior arrays, then
-    // edge-extended into halo'd volumes and turned into model1..7.
-    std::vector<float> defaults[7];
+    // The given host parameter arrays go to one dense device buffer (plus a
+    // flag word), one kernel builds every model volume from it, and the
+    // stream is synchronized once, to read the flag and release the buffer.
     const float* src[7] = {vp, eps, delta, vs, theta, phi, rho};
-    const float dflt[7] = {0, 0, 0, 0, 0, 0, 1};
-    for (int k = 1; k < 7; ++k)
-        if (!src[k]) {
-            defaults[k].assign(n, dflt[k]);
-            src[k] = defaults[k].data();
-        }
-    bool vti = true;
-    for (int64_t i = 0; i < n && vti; ++i) vti = (src[4][i] == 0.0f);
-    s->vti = vti;
-    float* dense = nullptr;
-    float* par[7] = {};
-    int rc = TTI_OK;
-    if (s->raw_alloc((void**)&dense, n * sizeof(float), st) != cudaSuccess) return cuda_rc(cudaGetLastError());
-    for (int k = 0; k < 7 && !rc; ++k) {
-        if (s->raw_alloc((void**)&par[k], s->nvol() * sizeof(float), st) != cudaSuccess) {
-            rc = cuda_rc(cudaGetLastError());
-            break;
-        }
-        if (cudaMemcpyAsync(dense, src[k], n * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess) {
-            rc = cuda_rc(cudaGetLastError());
-            break;
-        }
-        k_scatter_extend<<<dim3((L.ldimx + 127) / 128, L.ldimy, L.ldimz), 128, 0, st>>>(par[k], dense, L);
-        rc = launch_status();
-        if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
+    int present = 0;
+    for (const float* p : src) present += p ? 1 : 0;
+    const size_t bytes = (size_t)present * n * sizeof(float) + 256;
+    unsigned char* buf = nullptr;
+    if (s->raw_alloc((void**)&buf, bytes, st) != cudaSuccess) {
+        cudaGetLastError();
+        return TTI_ENOMEM;
     }
-    if (!rc)
-        rc = tti_launch_init_cijs(par[0], par[1], par[2], par[3], par[4], par[5], s->mv[1], s->mv[2], s->mv[3],
-                                  s->mv[4], s->mv[5], s->mv[6], s->mv[7], s->nvol(), st);
+    int* flag = reinterpret_cast<int*>(buf);
+    float* dense = reinterpret_cast<float*>(buf + 256);
+    ModelIn in{};
+    ModelOut out{};
+    for (int k = 0; k < 8; ++k) out.v[k] = s->mv[k];
+    int rc = cuda_rc(cudaMemsetAsync(flag, 0, sizeof(int), st));
+    for (int k = 0, j = 0; k < 7 && !rc; ++k) {
+        if (!src[k]) continue;
+        float* dst = dense + (size_t)j++ * n;
+        rc = cuda_rc(cudaMemcpyAsync(dst, src[k], n * sizeof(float), cudaMemcpyHostToDevice, st));
+        in.p[k] = dst;
+    }
     if (!rc) {
-        // buoyancy irho = 1/rho (the reference leaves Model11 unset, kernel_type2.cu:136-141)
-        std::vector<float> irho(n);
-        for (int64_t i = 0; i < n; ++i) irho[i] = 1.0f / src[6][i];
-        if (cudaMemcpyAsync(dense, irho.data(), n * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess)
-            rc = cuda_rc(cudaGetLastError());
-        if (!rc) {
-            k_scatter_extend<<<dim3((L.ldimx + 127) / 128, L.ldimy, L.ldimz), 128, 0, st>>>(s->mv[0], dense, L);
-            rc = launch_status();
-        }
-        if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
+        k_model_setup<<<dim3((L.ldimx + 127) / 128, L.ldimy, L.ldimz), 128, 0, st>>>(out, in, L, flag);
+        rc = launch_status();
     }
-    cudaFreeAsync(dense, st);
-    for (float* p : par)
-        if (p) cudaFreeAsync(p, st);
-    if (!rc) rc = cuda_rc(cudaStreamSynchronize(st));
-    else cudaStreamSynchronize(st);
-    if (!rc) s->model_set = true;
-    return rc;
+    int tti_flag = 0;
+    if (!rc) rc = cuda_rc(cudaMemcpyAsync(&tti_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    cudaFreeAsync(buf, st);
+    const int rs = cuda_rc(cudaStreamSynchronize(st));
+    if (!rc) rc = rs;
+    if (rc) return rc;
+    s->vti = (tti_flag == 0);
+    s->model_set = true;
+    return TTI_OK;
 }
 
 int tti_sim_set_source(tti_sim* s, int ix, int iy, int iz, const float* w, int nt)

@@ -296,9 +296,10 @@ int tti_launch_type1_adj(float* field3, float* field4, const float* field1, cons
         return TTI_EINVAL;
     if (use_sponge && (!ABx || !ABy || !ABz)) return TTI_EINVAL;
     const size_t nelem = (size_t)ldimx * ldimy * (size_t)(izend + 1 + kRadius);
-    float4* base = library_scratch(nelem);
-    if (!base) return TTI_ENOMEM;
     cudaStream_t st = S(stream);
+    const tti::CallScratch scratch(nelem, st);
+    float4* base = scratch.get();
+    if (!base) return TTI_ENOMEM;
     int rc = launch_base(field1, field2, model1, model2, model3, model4, base, ixbeg, ixend, iybeg, iyend, izbeg,
                          izend, ldimx, ldimy, st);
     if (rc) return rc;

@@ -272,7 +272,141 @@ DKEYS = ("d1x", "d1y", "d1z", "d2x", "d2y", "d2z")
 MKEYS = ("irho", "m1", "m2", "m3", "m4", "rx", "ry", "rz")
 
 
+def extend_to_layout(lay: Layout, a) -> np.ndarray:
+    """Interior array of shape (nz, ny, nx) spread over the halo'd layout by
+    repeating the nearest interior cell on every axis (x padding included)."""
+    a = np.asarray(a, np.float32).reshape(lay.nz, lay.ny, lay.nx)
+    r = RADIUS
+    return np.ascontiguousarray(np.pad(a, ((r, r), (r, r), (r, lay.ldimx - lay.nx - r)), mode="edge"))
+
+
+def models_from_parameters(lay: Layout, vp, eps=None, delta=None, vs=None, theta=None, phi=None, rho=None,
+                           dtype=np.float32) -> dict:
+    """Model volumes (irho, m1..m4, rx, ry, rz) from interior parameter arrays
+    of shape (nz, ny, nx), built on the host the way the simulator defines
+    its model set-up: every parameter is extended into the halo'd layout by
+    repeating the nearest interior cell, the reference's per-cell
+    ``init_cijs`` (simulator2SetUp.cu:10-29) maps (vp, eps, delta, vs, theta,
+    phi) to model1..model7, and the buoyancy is irho = 1/rho in FP32 (the
+    reference never sets Model11, kernel_type2.cu:136-141).  Missing
+    parameters default to 0 (rho to 1)."""
+    shape = (lay.nz, lay.ny, lay.nx)
+    par = [np.zeros(shape, np.float32) if a is None else a for a in (eps, delta, vs, theta, phi)]
+    full = [extend_to_layout(lay, a) for a in (vp, *par)]
+    m1, m2, m3, m4, rx, ry, rz = Oracle("f32").init_cijs(*full)
+    rho = np.ones(shape, np.float32) if rho is None else np.asarray(rho, np.float32)
+    irho = extend_to_layout(lay, np.float32(1.0) / rho)
+    out = dict(irho=irho, m1=m1, m2=m2, m3=m3, m4=m4, rx=rx, ry=ry, rz=rz)
+    return {k: np.ascontiguousarray(v, dtype) for k, v in out.items()}
+
+
 def new_state(lay: Layout, dtype=np.float32):
     st = {k: lay.zeros(dtype) for k in ("f1", "f2", "f3", "f4", "rhs3", "rhs4")}
     st["d"] = {k: lay.zeros(dtype) for k in DKEYS}
     return st
+
+
+def sponge_profile(n: int, ldim: int, width: int, absorb_low: bool):
+    """The simulator's sponge (A,B) pairs per global index (host logic mirror)."""
+    ab = np.ones((ldim, 2), np.float32)
+    for k in range(min(width, n)):
+        g = np.float32(np.exp(-((0.3 * (width - k) / width) ** 2)))
+        if absorb_low:
+            ab[RADIUS + k] = g
+        ab[RADIUS + n - 1 - k] = np.minimum(ab[RADIUS + n - 1 - k], g)
+    return np.ascontiguousarray(ab.reshape(-1))
+
+
+def rtm_shot(o, lay, m, ab, cfg, src, wavelet, rec, residual=None, adjoint=True, observed=None):
+    """Reference-order RTM with the oracle: forward with snapshots every
+    xcorr_step steps, adjoint driven by residual traces, Vp image and density
+    gradient at snapshot steps (simulator2SetUp.cu:517-782 with nsub = 1).
+    With ``observed`` the residual is the oracle's own traces minus it (the
+    simulator's adjoint_observed)."""
+    dt = np.float32(cfg.dt)
+    h = (cfg.dx, cfg.dy, cfg.dz)
+    g = o.grid(lay, dt, h, free_surface=cfg.free_surface, sponge_active=cfg.sponge_width > 0)
+    st = new_state(lay, o.dtype)
+    nrec = len(rec)
+    traces = np.zeros((cfg.nt, nrec), o.dtype)
+    snaps = {}
+    I = lay.interior
+    for n in range(cfg.nt):
+        row = np.zeros(nrec, o.dtype)
+        o.fwd_step(g, st, m, ab, src, float(wavelet[n]), rec, row)
+        traces[n] = row
+        if adjoint and n % cfg.xcorr_step == 0:
+            snaps[n] = [st[k][I].copy() for k in ("f3", "f4", "f1", "f2")]
+    out = {"traces": traces, "f3": st["f3"].copy(), "f4": st["f4"].copy()}
+    if not adjoint:
+        return out
+    if observed is not None:
+        res = (traces - np.asarray(observed, o.dtype)).astype(o.dtype)
+    else:
+        res = traces if residual is None else residual.astype(o.dtype)
+    adj = new_state(lay, o.dtype)
+    n_in = lay.nx * lay.ny * lay.nz
+    gvp = np.zeros(n_in, o.dtype)
+    grho = np.zeros(n_in, o.dtype)
+    for n in range(cfg.nt - 1, -1, -1):
+        o.adj_step(g, adj, m, ab, rec, np.ascontiguousarray(res[n]))
+        if n % cfg.xcorr_step == 0:
+            s3, s4, s1, s2 = snaps[n]
+            o.update_vp_gradient(lay, np.ascontiguousarray(s3.ravel()), np.ascontiguousarray(s4.ravel()),
+                                 gvp, adj["f3"], adj["f4"])
+            p, q = lay.zeros(o.dtype), lay.zeros(o.dtype)
+            p[I] = s1
+            q[I] = s2
+            if cfg.free_surface:
+                o.loop4(lay, p, q)
+            d = {k: lay.zeros(o.dtype) for k in DKEYS}
+            o.fwd_drv(lay, p, q, m["irho"], d, tuple(np.float32(1.0 / v) for v in h))
+            if cfg.free_surface:
+                o.loop4_derivatives(lay, d)
+            o.rho_gradient(lay, grho, d, adj["f1"], adj["f2"], m, h, lay.nx, lay.ny)
+    o.finalize_vp_gradient(lay, m["m3"], gvp, np.float32(cfg.dt * cfg.xcorr_step))
+    out["grad_vp"] = gvp.reshape(lay.nz, lay.ny, lay.nx)
+    out["grad_rho"] = grho.reshape(lay.nz, lay.ny, lay.nx)
+    return out
+
+
+def rtm_shot_t1(o, lay, m, ab, cfg, src, wavelet, rec, residual=None):
+    """RTM with the centred constant-density operator (scheme 1), composed
+    from the oracle's type1 restatement in the simulator's step order:
+    forward step: loop2, loop4, fwd_main_loop_2_1 (sponge form when the
+    sponge is on), source, receivers; adjoint step: residual injection,
+    adj_main_loop_2, loop2, loop4; Vp image (update_grad_loop) at snapshot
+    steps, then the simulator's Vp finalisation."""
+    dt = np.float32(cfg.dt)
+    h = (cfg.dx, cfg.dy, cfg.dz)
+    sponge = cfg.sponge_width > 0
+    f1, f2, f3, f4 = (lay.zeros() for _ in range(4))
+    nrec = len(rec)
+    traces = np.zeros((cfg.nt, nrec), np.float32)
+    snaps = {}
+    I = lay.interior
+    for n in range(cfg.nt):
+        o.loop2(lay, f1, f2, f3, f4, ab[0], ab[1], ab[2], dt)
+        if cfg.free_surface:
+            o.loop4(lay, f1, f2)
+        o.t1_fwd(lay, f3, f4, f1, f2, m, ab, dt, h, 1 if sponge else 0)
+        if src >= 0:
+            f3.flat[src] += np.float32(wavelet[n]) * dt
+            f4.flat[src] += np.float32(wavelet[n]) * dt
+        traces[n] = -(2 * f1.flat[rec] + f2.flat[rec]) / np.float32(3)
+        if n % cfg.xcorr_step == 0:
+            snaps[n] = (np.ascontiguousarray(f3[I].ravel()), np.ascontiguousarray(f4[I].ravel()))
+    res = (traces if residual is None else residual).astype(np.float32)
+    a1, a2, a3, a4 = (lay.zeros() for _ in range(4))
+    gvp = np.zeros(lay.nx * lay.ny * lay.nz, np.float32)
+    for n in range(cfg.nt - 1, -1, -1):
+        a3.flat[rec] += np.float32(-2.0 / 3.0) * res[n]
+        a4.flat[rec] += np.float32(-1.0 / 3.0) * res[n]
+        o.t1_adj(lay, a3, a4, a1, a2, m, ab, dt, h, sponge)
+        o.loop2(lay, a1, a2, a3, a4, ab[0], ab[1], ab[2], dt)
+        if cfg.free_surface:
+            o.loop4(lay, a1, a2)
+        if n % cfg.xcorr_step == 0:
+            o.t1_grad(lay, snaps[n][0], snaps[n][1], gvp, a3, a4)
+    o.finalize_vp_gradient(lay, m["m3"], gvp, np.float32(cfg.dt * cfg.xcorr_step))
+    return {"traces": traces, "f3": f3, "grad_vp": gvp.reshape(lay.nz, lay.ny, lay.nx)}

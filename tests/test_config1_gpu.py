@@ -9,7 +9,7 @@ import pytest
 import miniappsforhpe_b200 as P
 from miniappsforhpe_b200 import earth_models as EM
 from oracle import Layout, Oracle
-from tests.helpers import oracle_rtm, rel_l2, sim_models, sponge_profile
+from tests.helpers import oracle_models, oracle_rtm, rel_l2, sponge_profile
 
 
 @pytest.mark.gpu
@@ -26,8 +26,8 @@ def test_config1_vti_forward_traces_match_oracle():
         sim.set_source(*src, w)
         sim.set_receivers(rec)
         tr = sim.forward()
-        m = sim_models(sim)
     lay = Layout(n, n, n)
+    m = oracle_models(lay, model)
     ab = (sponge_profile(n, lay.ldimx, 20, True), sponge_profile(n, lay.ldimy, 20, True),
           sponge_profile(n, lay.ldimz, 20, False))
     rec_idx = np.array([lay.index(*r) for r in rec], np.int64)

@@ -13,7 +13,7 @@ import pytest
 import miniappsforhpe_b200 as P
 from miniappsforhpe_b200 import earth_models as EM
 from oracle import Layout, Oracle
-from tests.helpers import oracle_rtm, rel_l2, report_dir, sim_models, sponge_profile
+from tests.helpers import oracle_models, oracle_rtm, rel_l2, report_dir, sponge_profile
 
 
 
@@ -27,8 +27,7 @@ def run(prec, model, nx, ny, nz, nt, dt, w, src, rec):
         tr = sim.forward()
         sim.adjoint(tr)
         gv, gr = sim.image()
-        m = sim_models(sim)
-    return cfg, tr, gv, gr, m
+    return cfg, tr, gv, gr
 
 
 @pytest.mark.gpu
@@ -40,15 +39,15 @@ def test_reduced_precision_snapshots_against_fp64_oracle():
     src = (nx // 2, ny // 2, 5)
     rec = EM.receiver_plane(nx, ny, 3)
     res = {p: run(p, model, nx, ny, nz, nt, dt, w, src, rec) for p in ("fp32", "fp16", "bf16")}
-    cfg, _, _, _, m32 = res["fp32"]
+    cfg = res["fp32"][0]
     lay = Layout(nx, ny, nz)
-    m64 = {k: v.astype(np.float64) for k, v in m32.items()}
+    m64 = oracle_models(lay, model, np.float64)
     ab = (sponge_profile(nx, lay.ldimx, 8, True), sponge_profile(ny, lay.ldimy, 8, True),
           sponge_profile(nz, lay.ldimz, 8, False))
     rec_idx = np.array([lay.index(*r) for r in rec], np.int64)
     want = oracle_rtm(Oracle("f64"), lay, m64, ab, cfg, lay.index(*src), w.astype(np.float64), rec_idx)
     report = {}
-    for p, (_, tr, gv, gr, _) in res.items():
+    for p, (_, tr, gv, gr) in res.items():
         report[p] = {"traces": rel_l2(tr, want["traces"]), "image_vp": rel_l2(gv, want["grad_vp"]),
                      "grad_rho": rel_l2(gr, want["grad_rho"])}
     print(json.dumps(report))
@@ -87,9 +86,9 @@ def test_reduced_precision_wavefields_against_fp64_oracle():
     w = EM.ricker(nt, dt, 25.0) * 1e3
     src = (nx // 2, ny // 2, 5)
     rec = EM.receiver_plane(nx, ny, 3)
-    cfg, _, _, _, m32 = run("fp32", model, nx, ny, nz, nt, dt, w, src, rec)
+    cfg = run("fp32", model, nx, ny, nz, nt, dt, w, src, rec)[0]
     lay = Layout(nx, ny, nz)
-    m64 = {k: v.astype(np.float64) for k, v in m32.items()}
+    m64 = oracle_models(lay, model, np.float64)
     ab = (sponge_profile(nx, lay.ldimx, 8, True), sponge_profile(ny, lay.ldimy, 8, True),
           sponge_profile(nz, lay.ldimz, 8, False))
     rec_idx = np.array([lay.index(*r) for r in rec], np.int64)
@@ -122,3 +121,54 @@ def test_reduced_precision_wavefields_recompute_exactly():
     ck = run_wave("fp16", *args, checkpoint_every=8)
     for a, b in zip(ck, plain):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_config3_128_vti_500_steps_against_fp64_oracle():
+    """The forward configuration (128^3 layered VTI, 20-cell sponge, 15 Hz
+    Ricker at (64, 64, 5), 500 steps, receivers on plane z = 3) as a full RTM
+    shot (imaging every 4 steps, the traces as residual) in plain FP32, with
+    FP16 / BF16 snapshots, and with FP16 / BF16 wavefields and snapshots,
+    against one FP64 oracle run of the same shot.  Every error is reported."""
+    n, nt = 128, 500
+    model = EM.layered_vti(n, n, n, nlayers=6, seed=1234)
+    dt = EM.cfl_dt(model, 10.0, cfl=0.4)
+    w = EM.ricker(nt, dt, 15.0)
+    src = (64, 64, 5)
+    rec = EM.receiver_plane(n, n, 3)
+
+    def shot(snap, wave):
+        cfg = P.Config(nx=n, ny=n, nz=n, dt=dt, nt=nt, xcorr_step=4, sponge_width=20, fused=True,
+                       snap_precision=snap, wave_precision=wave)
+        with P.Simulator(cfg) as sim:
+            sim.set_model(**model)
+            sim.set_source(*src, w)
+            sim.set_receivers(rec)
+            tr = sim.forward()
+            sim.adjoint(tr)
+            gv, gr = sim.image()
+        return cfg, tr, gv, gr
+
+    forms = {"fp32": ("fp32", "fp32"), "snap_fp16": ("fp16", "fp32"), "snap_bf16": ("bf16", "fp32"),
+             "wave_fp16": ("fp16", "fp16"), "wave_bf16": ("bf16", "bf16")}
+    res = {k: shot(*v) for k, v in forms.items()}
+    cfg = res["fp32"][0]
+    lay = Layout(n, n, n)
+    ab = (sponge_profile(n, lay.ldimx, 20, True), sponge_profile(n, lay.ldimy, 20, True),
+          sponge_profile(n, lay.ldimz, 20, False))
+    rec_idx = np.array([lay.index(*r) for r in rec], np.int64)
+    want = oracle_rtm(Oracle("f64"), lay, oracle_models(lay, model, np.float64), ab, cfg, lay.index(*src),
+                      w.astype(np.float64), rec_idx)
+    report = {"config": "128^3 layered VTI, 500 steps, imaging every 4, vs FP64 oracle"}
+    for k, (_, tr, gv, gr) in res.items():
+        assert np.all(np.isfinite(tr)) and np.all(np.isfinite(gv)) and np.all(np.isfinite(gr)), k
+        report[k] = {"traces": rel_l2(tr, want["traces"]), "image_vp": rel_l2(gv, want["grad_vp"]),
+                     "grad_rho": rel_l2(gr, want["grad_rho"])}
+    print(json.dumps(report))
+    if report_dir():
+        with open(os.path.join(report_dir(), "precision_report_config3.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    assert max(report["fp32"].values()) < 1e-5
+    assert report["snap_fp16"]["image_vp"] < 1e-3 and report["snap_fp16"]["grad_rho"] < 1e-3
+    for k in ("snap_bf16", "wave_fp16", "wave_bf16"):
+        assert max(report[k].values()) < 5e-2, (k, report[k])

@@ -13,7 +13,7 @@ import pytest
 import miniappsforhpe_b200 as P
 from miniappsforhpe_b200 import earth_models as EM
 from oracle import Layout, Oracle
-from tests.helpers import oracle_rtm, rel_l2, sim_models, sponge_profile
+from tests.helpers import oracle_models, oracle_rtm, rel_l2, sponge_profile
 
 
 def make_sim(nx, ny, nz, tti, fused, fs=True, sponge=6, nt=48, xcorr=4, seed=5):
@@ -45,7 +45,7 @@ def test_reference_sequence_matches_oracle(tti):
     sim.adjoint(res)
     gvp, grho = sim.image()
     lay = Layout(nx, ny, nz)
-    m = sim_models(sim)
+    m = oracle_models(lay, model)
     ab = (sponge_profile(nx, lay.ldimx, cfg.sponge_width, True),
           sponge_profile(ny, lay.ldimy, cfg.sponge_width, True),
           sponge_profile(nz, lay.ldimz, cfg.sponge_width, not cfg.free_surface))

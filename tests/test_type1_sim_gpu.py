@@ -15,7 +15,7 @@ import pytest
 import miniappsforhpe_b200 as P
 from miniappsforhpe_b200 import earth_models as EM
 from oracle import Layout, Oracle
-from tests.helpers import oracle_rtm_t1, rel_l2, sim_models, sponge_profile
+from tests.helpers import oracle_models, oracle_rtm_t1, rel_l2, sponge_profile
 
 
 def make_sim(nx, ny, nz, tti, fused, fs=True, sponge=6, nt=40, xcorr=4, seed=7, **kw):
@@ -33,7 +33,7 @@ def make_sim(nx, ny, nz, tti, fused, fs=True, sponge=6, nt=40, xcorr=4, seed=7, 
     sim.set_source(*src, w)
     rec = EM.receiver_plane(nx, ny, 3)
     sim.set_receivers(rec)
-    return sim, cfg, w, src, rec
+    return sim, cfg, w, src, rec, model
 
 
 def rtm(sim, residual=None):
@@ -47,14 +47,14 @@ def rtm(sim, residual=None):
 @pytest.mark.parametrize("tti", [False, True], ids=["vti", "tti"])
 def test_type1_sequence_matches_oracle(tti):
     nx, ny, nz = 36, 30, 28
-    sim, cfg, w, src, rec = make_sim(nx, ny, nz, tti, fused=False, nt=32)
+    sim, cfg, w, src, rec, model = make_sim(nx, ny, nz, tti, fused=False, nt=32)
     tr = sim.forward()
     rng = np.random.default_rng(4)
     res = (tr * rng.uniform(0.5, 1.5, tr.shape)).astype(np.float32)
     sim.adjoint(res)
     gvp, grho = sim.image()
     lay = Layout(nx, ny, nz)
-    m = sim_models(sim)
+    m = oracle_models(lay, model)
     ab = (sponge_profile(nx, lay.ldimx, cfg.sponge_width, True),
           sponge_profile(ny, lay.ldimy, cfg.sponge_width, True),
           sponge_profile(nz, lay.ldimz, cfg.sponge_width, not cfg.free_surface))
@@ -110,7 +110,7 @@ def test_type1_dot_product(tti):
     """<F s, r> = <s, F^T r> for the receiver map of the fused type1 forward
     and adjoint (no free surface, no sponge)."""
     nt = 60
-    sim, cfg, w, src, rec = make_sim(48, 40, 44, tti, fused=True, fs=False, sponge=0, nt=nt)
+    sim, cfg, w, src, rec, _ = make_sim(48, 40, 44, tti, fused=True, fs=False, sponge=0, nt=nt)
     rng = np.random.default_rng(10)
     s = rng.standard_normal(nt).astype(np.float32)
     sim.set_source(*src, s)

@@ -67,3 +67,33 @@ def test_noalloc_adjoint_derivatives_match_the_allocating_entry_point():
                  lay.ldimx, lay.ldimy, 8, 1e-3, 1.0, 1.0, 1.0, None)
     assert rc == P.ETOOBIG
     assert P.status_string(rc) == "request exceeds a fixed-capacity buffer"
+
+
+@pytest.mark.gpu
+def test_noalloc_calls_leave_free_device_memory_unchanged():
+    """The point of the entry point: after one warm-up call (which loads the
+    kernels and looks up the array's address), further calls, with no
+    allocating call in between, do not change the device's free memory."""
+    import torch
+    noalloc = entry("tti_launch_adj_kernel2_drv_noalloc")
+    lay = Layout(40, 36, 30)
+    rng = np.random.default_rng(13)
+    m = random_model(lay, rng, tti=True)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    f1, f2 = dev(random_field(lay, rng)), dev(random_field(lay, rng))
+    mv = {k: dev(v) for k, v in m.items()}
+    outs = [torch.zeros(lay.shape, dtype=torch.float32, device="cuda") for _ in range(8)]
+    xb, xe, yb, ye, zb, ze = lay.ranges
+    args = ([o.data_ptr() for o in outs] + [f1.data_ptr(), f2.data_ptr()] +
+            [mv[k].data_ptr() for k in ("irho", "m1", "m2", "m3", "m4", "rx", "ry", "rz")] +
+            [xb, xe, yb, ye, zb, ze, 0.01, 0.01, 0.01, 0.0025, 0.0025, 0.0025, lay.ldimx, lay.ldimy, 8, 1e-3,
+             0.1, 0.1, 0.1, None])
+    assert noalloc(*args) == P.OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        assert noalloc(*args) == P.OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert np.abs(outs[0].cpu().numpy()).max() > 0
