@@ -56,6 +56,24 @@ constexpr int PW = TX + 16, PH = TY + 16;  // p/q tile with a halo of 8
 constexpr int IW = TX + 8, IH = TY + 8;    // tile with a halo of 4
 constexpr int LAG = 7;                     // output plane = arrival plane - 7
 
+// Packed pairs: the two wavefields of a cell travel together in one float2
+// and are updated by the paired FP32 instructions of sm_100 (FFMA2, FADD2,
+// FMUL2), one instruction for both fields with per-component rounding the
+// same as fmaf / add / mul.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// Reciprocal of a buoyancy (irho in (0, 1]): the hardware approximation,
+// within one unit in the last place.
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // TMA / mbarrier primitives (PTX ISA 8.x, sm_90+).
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -97,12 +115,43 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
     }
     return true;
 }
+// Give-up path of a pipelined CTA.  A bounded wait that times out sets the
+// error word and the waiting thread's `dead` flag; the CTA agrees to stop at
+// its next block barrier (__syncthreads_or of the flags), so no thread
+// issues a further load or processes a further plane.  Before exiting,
+// thread 0 waits, again with a bound, for every plane it issued from the
+// one being waited on when the CTA stopped (global plane g: stage g % ns,
+// parity (g / ns) & 1; at most the prefetch distance ahead, so one phase
+// per stage) so that no bulk copy it started is left writing into shared
+// memory.  If such a copy never completes even then, the CTA exits with it
+// in flight; what the copy does afterwards is undefined, and the error word
+// already tells the host that the launch's results are invalid.
+__device__ __noinline__ void drain_loads(uint64_t* bars, int ns, int g0, int g1)
+{
+    for (int g = g0; g < g1; ++g) {
+        uint64_t* b = &bars[g % ns];
+        const uint32_t par = (uint32_t)((g / ns) & 1);
+        const long long t0 = clock64();
+        while (!mbar_try_wait(b, par))
+            if (clock64() - t0 > (2LL << 30)) break;
+    }
+}
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar)
 {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
         "[%5];" ::"r"(saddr(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(saddr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
+                                            uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(saddr(bar))
         : "memory");
 }
 
@@ -164,7 +213,8 @@ struct WorkRange {
 // <= izbeg instead take the value at 2*izbeg+1-pos (kernel_type2_small.cu:
 // 34-39), which is in the queue itself for the four outputs nearest the
 // surface: j' = 7 - 2*(z-izbeg) - j.
-__device__ __forceinline__ void resolve_dz(float (&q)[8], int dtop)
+template <typename T>
+__device__ __forceinline__ void resolve_dz(T (&q)[8], int dtop)
 {
     switch (dtop) {
     case 0:
@@ -212,6 +262,15 @@ struct FwdParams {
     int* err;
     int wave_prec;            // 0, or p/q rounded to FP16 (1) / BF16 (2) each step
     const float* wave_scale;  // 2 scales (p, q) of this step's output
+    // stencil coefficients with the grid spacings folded in, as (c, c) pairs
+    float2 kd[3][4];    // c1(i)/dx, /dy, /dz, i = 1..4 (staggered D-)
+    float2 ktap[3][8];  // tap(k)/dx, /dy, /dz, k = 0..7 (staggered D+ over consecutive points)
+    float2 kzm[8];      // D- z scatter into queue slot j: +c1(4-j)/dz (j <= 3), -c1(j-3)/dz
+    float2 kzx[9];      // c2(|m|)/(4 dz dx) for plane offset m = -4..4
+    float2 kyz[9];      // c2(|m|)/(4 dy dz)
+    float2 kxy[9];      // c2(|k|)/(4 dx dy) for diagonal offset k = -4..4
+    const float4* ma;   // (m1, m2, m3, m4) per cell
+    const float4* mb;   // (irho, rx, ry, rz) per cell (TTI)
 };
 
 constexpr int FWD_NS = 11;  // ring: planes L-8 .. L+2
@@ -239,6 +298,8 @@ __global__ void __launch_bounds__(NT, 1)
     const Layout& L = a.L;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     bool dead = false;
+    bool stop = false;             // the CTA gave up (a bounded wait timed out)
+    int g_issued = 0, g_wait = 0;  // planes issued (thread 0) / plane last waited on
 
     if (tid == 0) {
         for (int s = 0; s < FWD_NS; ++s) mbar_init(&bars[s], 1);
@@ -256,9 +317,13 @@ __global__ void __launch_bounds__(NT, 1)
     const int ntot = sg.len + 2 * LAG;  // arrival planes zs-7 .. ze+7
     const int x = x0 + tx, y = y0 + ty;
     const bool owner = (x <= L.ixend) && (y <= L.iyend);
-    __syncthreads();  // barriers initialised; the previous segment is done with the ring
+    if (__syncthreads_or(dead)) {  // barriers initialised; the previous segment is done with the ring
+        stop = true;
+        break;
+    }
 
     auto issue = [&](int t) {
+        ++g_issued;
         const int s = (gbase + t) % FWD_NS, z = zs - LAG + t;
         float* dst = ring + (size_t)s * 2 * PH * PW;
         mbar_expect_tx(&bars[s], (uint32_t)(FWD_SLOT_P + FWD_SLOT_I));
@@ -283,11 +348,15 @@ __global__ void __launch_bounds__(NT, 1)
 
     auto back = [&](int k) { const int v = s - k; return v < 0 ? v + FWD_NS : v; };
     for (int t = 0; t < ntot; ++t) {
-        __syncthreads();  // every thread is done with iteration t-1
+        if (__syncthreads_or(dead)) {  // every thread is done with iteration t-1
+            stop = true;
+            break;
+        }
         if (tid == 0 && t + FWD_PF < ntot) {
             fence_proxy_async();
             issue(t + FWD_PF);
         }
+        g_wait = gbase + t;
         mbar_wait(&bars[s], phase, a.err, dead);
         const int Lz = zs - LAG + t;
         const float* P1 = ring + (size_t)s * 2 * PH * PW;
@@ -543,7 +612,9 @@ __global__ void __launch_bounds__(NT, 1)
             phase ^= 1u;
         }
     }
+    if (stop) break;
     }  // segments
+    if (stop && tid == 0) drain_loads(bars, FWD_NS, g_wait, g_issued);
     // one atomic per warp and field for all segments; the next
     // snapshot's scale is taken from this running max
     if (a.snap && a.snap_prec != SNAP_F32) {
@@ -556,14 +627,22 @@ __global__ void __launch_bounds__(NT, 1)
 }
 
 
+
 // ---------------------------------------------------------------------------
 // Fused adjoint step (one reference adjoint step: adj_drv, loop4_derivatives,
 // update_adj_kernel_main_3, loop2, loop4).  The transposed model is applied
 // before the derivatives (kernel_type2_grad_snap.cu:98-129), so every term of
 // an output cell is a plain sum and the terms are accumulated in per-thread
-// queues as the planes arrive: the x+y part when plane z arrives, the mixed
-// part plane by plane from z-4 to z+4 (the reference's order), the z part when
-// plane z+7 arrives.
+// queues as the planes arrive: the x+y and xy parts when plane z arrives,
+// the yz/zx part plane by plane from z-4 to z+4 (the reference's order), the
+// z part when plane z+7 arrives.
+//
+// Each staged plane holds p and q, and the model as two interleaved float4
+// volumes, (m1, m2, m3, m4) and (irho, rx, ry, rz) (VTI: irho alone), all
+// with a halo of 8, so a staging position's nine model values are two
+// 128-bit shared loads.  The transposed-model temporaries of a plane are
+// formed once per staging position that needs them, in passes whose role
+// (which temporaries a position feeds) is uniform per warp.
 struct AdjParams {
     float* pout;
     float* qout;
@@ -577,20 +656,25 @@ struct AdjParams {
     int ztop;
     int fs;
     int sponge;
-    float dt, invdx, invdy, invdz, invdxy, invdyz, invdzx;
+    float dt;
     int* err;
     int wave_prec;            // 0, or p/q rounded to FP16 (1) / BF16 (2) each step
     const float* wave_scale;  // 2 scales (p, q) of this step's output
+    // stencil coefficients with the grid spacings folded in, as (c, c) pairs
+    float2 kd[3][4];  // c1(i)/dx, /dy, /dz, i = 1..4 (staggered D- and D+)
+    float2 kzm[8];    // D- z scatter into queue slot j: +c1(4-j)/dz (j <= 3), -c1(j-3)/dz
+    float2 kyz[9];    // sign(i) c2(|i|)/(4 dy dz) for plane offset i = -4..4
+    float2 kzx[9];    // sign(i) c2(|i|)/(4 dz dx)
+    float2 kxy[4];    // c2(k)/(4 dx dy), k = 1..4
 };
 
-// Staging per plane: p, q, m1, m2, m3, m4, irho, rx, ry with a halo of 8 and
-// rz with a halo of 4.
+// Staging per plane: p, q (float), MA = (m1, m2, m3, m4) and MB = (irho, rx,
+// ry, rz) (float4; VTI: irho as float), each PW x PH (halo 8).
 constexpr int ADJ_NSTAGE = 3;
 constexpr int ADJ_PF = 2;
-constexpr int ADJ_NARR = 9;
-constexpr size_t ADJ_ARR = (size_t)PH * PW * sizeof(float);
-constexpr size_t ADJ_RZ = (size_t)IH * IW * sizeof(float);
-constexpr size_t ADJ_STAGE = ADJ_NARR * ADJ_ARR + ADJ_RZ;
+constexpr size_t ADJ_F1 = (size_t)PH * PW * sizeof(float);
+constexpr size_t ADJ_F4 = (size_t)PH * PW * sizeof(float4);
+__host__ __device__ constexpr size_t adj_stage(bool tti) { return 2 * ADJ_F1 + ADJ_F4 + (tti ? ADJ_F4 : ADJ_F1); }
 constexpr size_t ADJ_TXX = (size_t)2 * TY * PW * sizeof(float);  // rows y0.., cols x0-8..
 constexpr size_t ADJ_TYY = (size_t)2 * PH * TX * sizeof(float);  // rows y0-8.., cols x0..
 constexpr size_t ADJ_TXY = (size_t)2 * IH * IW * sizeof(float);  // rows y0-4.., cols x0-4..
@@ -598,41 +682,26 @@ constexpr size_t ADJ_TYZ = (size_t)2 * IH * TX * sizeof(float);  // rows y0-4..,
 constexpr size_t ADJ_TZX = (size_t)2 * TY * IW * sizeof(float);  // rows y0.., cols x0-4..
 constexpr size_t ADJ_DX = (size_t)2 * TY * IW * sizeof(float);   // rows y0.., cols x0-4..
 constexpr size_t ADJ_DY = (size_t)2 * IH * TX * sizeof(float);   // rows y0-4.., cols x0..
-constexpr size_t ADJ_SMEM = ADJ_NSTAGE * ADJ_STAGE + ADJ_TXX + ADJ_TYY + ADJ_TXY + ADJ_TYZ + ADJ_TZX + ADJ_DX +
-                            ADJ_DY + ADJ_NSTAGE * sizeof(uint64_t);
+__host__ __device__ constexpr size_t adj_smem(bool tti)
+{
+    return ADJ_NSTAGE * adj_stage(tti) + ADJ_TXX + ADJ_TYY + ADJ_TXY + ADJ_TYZ + ADJ_TZX + ADJ_DX + ADJ_DY +
+           ADJ_NSTAGE * sizeof(uint64_t);
+}
+static_assert(adj_smem(true) <= 227 * 1024, "adjoint staging and tiles fit one CTA's shared memory");
 
 struct AdjMaps {
-    CUtensorMap m[ADJ_NARR];  // p, q, m1, m2, m3, m4, irho, rx, ry  (box PW x PH)
-    CUtensorMap rz;           // box IW x IH
+    CUtensorMap p, q;  // box PW x PH
+    CUtensorMap ma;    // 4D (4, x, y, z), box 4 x PW x PH
+    CUtensorMap mb;    // TTI: 4D like ma; VTI: irho, box PW x PH
 };
-
-enum { S_P = 0, S_Q, S_M1, S_M2, S_M3, S_M4, S_IR, S_RX, S_RY };
-
-// Point-wise transposed model at staging offset k:
-//   s1 = m1 p + m2 q, h1 = (-m1 + m4) p - m2 q, s2 = m4 q, h2 = m2 p + (-m4 + m3) q.
-struct Base {
-    float s1, h1, s2, h2, rho;
-};
-__device__ __forceinline__ Base base_at(const float* st, int k)
-{
-    const float p = st[S_P * PH * PW + k], q = st[S_Q * PH * PW + k];
-    const float a1 = st[S_M1 * PH * PW + k], a2 = st[S_M2 * PH * PW + k], a3 = st[S_M3 * PH * PW + k],
-                a4 = st[S_M4 * PH * PW + k];
-    Base b;
-    b.s1 = a1 * p + a2 * q;
-    b.h1 = (-a1 + a4) * p - a2 * q;
-    b.s2 = a4 * q;
-    b.h2 = a2 * p + (-a4 + a3) * q;
-    b.rho = __frcp_rn(st[S_IR * PH * PW + k]);
-    return b;
-}
 
 template <bool TTI>
 __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__ AdjMaps tm, const AdjParams a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    float* stage = reinterpret_cast<float*>(smem);
-    unsigned char* sp = smem + ADJ_NSTAGE * ADJ_STAGE;
+    constexpr size_t STAGE = adj_stage(TTI);
+    unsigned char* stage = smem;
+    unsigned char* sp = smem + ADJ_NSTAGE * STAGE;
     // temporaries and derivative tiles: both fields of a cell side by side
     float2* txx = reinterpret_cast<float2*>(sp);  // [TY][PW]
     sp += ADJ_TXX;
@@ -652,9 +721,10 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
 
     const Layout& L = a.L;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int warp = tid >> 5, lane = tid & 31;
     bool dead = false;
-    constexpr int NLOAD = TTI ? ADJ_NARR : S_RX;  // VTI: rx, ry, rz are not read
-    constexpr uint32_t TX_BYTES = (uint32_t)(NLOAD * ADJ_ARR + (TTI ? ADJ_RZ : 0));
+    bool stop = false;             // the CTA gave up (a bounded wait timed out)
+    int g_issued = 0, g_wait = 0;  // planes issued (thread 0) / plane last waited on
 
     if (tid == 0) {
         for (int s = 0; s < ADJ_NSTAGE; ++s) mbar_init(&bars[s], 1);
@@ -669,35 +739,42 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
     const int ntot = sg.len + 2 * LAG;
     const int x = x0 + tx, y = y0 + ty;
     const bool owner = (x <= L.ixend) && (y <= L.iyend);
-    __syncthreads();  // barriers initialised; the previous segment is done with the stages
+    if (__syncthreads_or(dead)) {  // barriers initialised; the previous segment is done with the stages
+        stop = true;
+        break;
+    }
 
     auto issue = [&](int t) {
-        const int s = (gbase + t) % ADJ_NSTAGE, z = zs - LAG + t;
-        float* dst = stage + (size_t)s * (ADJ_STAGE / sizeof(float));
-        mbar_expect_tx(&bars[s], TX_BYTES);
-#pragma unroll
-        for (int k = 0; k < NLOAD; ++k) tma_load_3d(dst + k * PH * PW, &tm.m[k], x0 - 8, y0 - 8, z, &bars[s]);
-        if constexpr (TTI) tma_load_3d(dst + ADJ_NARR * PH * PW, &tm.rz, x0 - 4, y0 - 4, z, &bars[s]);
+        ++g_issued;
+        const int sl = (gbase + t) % ADJ_NSTAGE, z = zs - LAG + t;
+        unsigned char* dst = stage + (size_t)sl * STAGE;
+        mbar_expect_tx(&bars[sl], (uint32_t)STAGE);
+        tma_load_3d(dst, &tm.p, x0 - 8, y0 - 8, z, &bars[sl]);
+        tma_load_3d(dst + ADJ_F1, &tm.q, x0 - 8, y0 - 8, z, &bars[sl]);
+        tma_load_4d(dst + 2 * ADJ_F1, &tm.ma, 0, x0 - 8, y0 - 8, z, &bars[sl]);
+        if constexpr (TTI)
+            tma_load_4d(dst + 2 * ADJ_F1 + ADJ_F4, &tm.mb, 0, x0 - 8, y0 - 8, z, &bars[sl]);
+        else
+            tma_load_3d(dst + 2 * ADJ_F1 + ADJ_F4, &tm.mb, x0 - 8, y0 - 8, z, &bars[sl]);
     };
     if (tid == 0)
         for (int t = 0; t < ADJ_PF && t < ntot; ++t) issue(t);
 
-    float dzq1[8], dzq2[8];  // D- partial sums, positions L-3 .. L+4
-    float dZ1[8], dZ2[8];    // buoyancy-scaled z derivatives, positions L-10 .. L-3
-    float mx1[12], mx2[12];  // mixed rhs, outputs L-7 .. L+4
-    float sxy1[8], sxy2[8];  // x+y parts, outputs L-7 .. L
-    float irq[4];            // buoyancy of this column, planes L-3 .. L
+    // register queues, both fields of a cell in one pair
+    float2 dzq[8];  // D- partial sums, positions L-3 .. L+4
+    float2 dZ[8];   // buoyancy-scaled z derivatives, positions L-10 .. L-3
+    float2 mq[8];   // yz/zx parts of outputs L-4 .. L+3 (before plane L)
+    float2 sxy[8];  // completed in-plane parts (x, y, xy, and yz/zx once complete), outputs L-7 .. L
+    float irq[4];   // buoyancy of this column, planes L-3 .. L
     const float2 sx = owner ? __ldg(a.abx + x) : make_float2(1.0f, 1.0f);
     const float2 sy = owner ? __ldg(a.aby + y) : make_float2(1.0f, 1.0f);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) dzq1[j] = dzq2[j] = dZ1[j] = dZ2[j] = sxy1[j] = sxy2[j] = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 12; ++j) mx1[j] = mx2[j] = 0.0f;
+    for (int j = 0; j < 8; ++j) dzq[j] = dZ[j] = mq[j] = sxy[j] = f2(0.0f);
 #pragma unroll
     for (int j = 0; j < 4; ++j) irq[j] = 0.0f;
 
     for (int t = 0; t < ntot; ++t) {
-        // Stage (t+2)%3 was last read in iteration t-1, before its final barrier.
+        // Stage (t+2)%3 was last read in iteration t-1, before its second barrier.
         if (tid == 0 && t + ADJ_PF < ntot) {
             fence_proxy_async();
             issue(t + ADJ_PF);
@@ -707,258 +784,250 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
         const int zo = Lz - LAG;
         const bool out_here = (zo >= zs) && owner;
         const int64_t go = L.idx(x, y, max(zo, 0));
-        float o3 = 0.0f, o4 = 0.0f, opc = 0.0f, oqc = 0.0f;
+        float2 o34 = f2(0.0f), opq = f2(0.0f);
         float2 osz = make_float2(1.0f, 1.0f);
         if (out_here) {
-            o3 = a.f3[go];
-            o4 = a.f4[go];
-            opc = __ldg(a.pin + go);
-            oqc = __ldg(a.qin + go);
+            o34 = make_float2(a.f3[go], a.f4[go]);
+            opq = make_float2(__ldg(a.pin + go), __ldg(a.qin + go));
             osz = __ldg(a.abz + zo);
         }
+        g_wait = gbase + t;
         mbar_wait(&bars[s], phase, a.err, dead);
-        const float* st = stage + (size_t)s * (ADJ_STAGE / sizeof(float));
-        const float* srz = st + ADJ_NARR * PH * PW;  // rz tile, origin (x0-4, y0-4)
+        const unsigned char* st = stage + (size_t)s * STAGE;
+        const float* SP = reinterpret_cast<const float*>(st);
+        const float* SQ = SP + PH * PW;
+        const float4* SMA = reinterpret_cast<const float4*>(st + 2 * ADJ_F1);
+        const float4* SMB = reinterpret_cast<const float4*>(st + 2 * ADJ_F1 + ADJ_F4);  // TTI
+        const float* SIR = reinterpret_cast<const float*>(st + 2 * ADJ_F1 + ADJ_F4);    // VTI
+        // transposed model at staging offset k (kernel_type2_grad_snap.cu:98-129):
+        // S = (m1 p + m2 q, m4 q), H = ((m4 - m1) p - m2 q, m2 p + (m3 - m4) q)
+        auto base = [&](int k, float2& S, float2& H) {
+            const float p = SP[k], q = SQ[k];
+            const float4 m = SMA[k];
+            S = fma2(make_float2(m.y, m.w), f2(q), make_float2(m.x * p, 0.0f));
+            H = fma2(make_float2(m.w - m.x, m.z - m.w), make_float2(p, q), make_float2(-(m.y * q), m.y * p));
+        };
+        // (irho, rx, ry, rz) at staging offset k
+        auto geo = [&](int k) {
+            if constexpr (TTI) return SMB[k];
+            else return make_float4(SIR[k], 0.0f, 0.0f, 1.0f);
+        };
 
-        // (1) temporaries of plane L (kernel_type2_grad_snap.cu:98-129), each
-        //     staging position visited once: position (r, c) of the halo-8
-        //     tile (y = y0-8+r, x = x0-8+c) feeds
-        //       xx if 8<=r<24;  yy if 8<=c<40;  xy if 4<=r<28 and 4<=c<44;
-        //       yz if 4<=r<28 and 8<=c<40;  zx if 8<=r<24 and 4<=c<44.
-        auto temps_at = [&](int r, int c) {
-            const bool nx_ = (r >= 8 && r < 8 + TY), ny_ = (c >= 8 && c < 8 + TX);
-            const bool in4 = (r >= 4 && r < PH - 4 && c >= 4 && c < PW - 4);
-            if (!(nx_ || ny_ || (TTI && in4))) return;
-            const int k = r * PW + c;
-            const Base b = base_at(st, k);
-            const float vrx = TTI ? st[S_RX * PH * PW + k] : 0.0f;
-            const float vry = TTI ? st[S_RY * PH * PW + k] : 0.0f;
-            if (nx_) {
-                const float rr = vrx * vrx;
-                txx[(r - 8) * PW + c] = make_float2(b.rho * (b.s1 + rr * b.h1), b.rho * (b.s2 + rr * b.h2));
-            }
-            if (ny_) {
-                const float rr = vry * vry;
-                tyy[r * TX + c - 8] = make_float2(b.rho * (b.s1 + rr * b.h1), b.rho * (b.s2 + rr * b.h2));
-            }
+        // (1) temporaries of plane L.  Position (r, c) of the staging tile
+        //     (y = y0-8+r, x = x0-8+c) feeds xx if 8<=r<24; yy if 8<=c<40;
+        //     xy if 4<=r<28 and 4<=c<44; yz if 4<=r<28 and 8<=c<40; zx if
+        //     8<=r<24 and 4<=c<44.
+        // core (r, c) = (ty+8, tx+8): all of them, and this column's zz
+        float2 tz;
+        float irc;  // buoyancy of this column at plane L
+        {
+            const int k = (ty + 8) * PW + tx + 8;
+            float2 S, H;
+            base(k, S, H);
+            const float4 g = geo(k);
+            irc = g.x;
+            const float2 rho = f2(rcp_approx(g.x));
+            txx[ty * PW + tx + 8] = mul2(rho, fma2(f2(g.y * g.y), H, S));
+            tyy[(ty + 8) * TX + tx] = mul2(rho, fma2(f2(g.z * g.z), H, S));
+            tz = mul2(rho, fma2(f2(g.w * g.w), H, S));
             if constexpr (TTI) {
-                if (in4) {
-                    const float vrz = srz[(r - 4) * IW + c - 4];
-                    const float wxy = 2.0f * vrx * vry;
-                    txy[(r - 4) * IW + c - 4] = make_float2(wxy * b.h1, wxy * b.h2);
-                    if (ny_) {
-                        const float w = 2.0f * vry * vrz;
-                        tyz[(r - 4) * TX + c - 8] = make_float2(w * b.h1, w * b.h2);
-                    }
-                    if (nx_) {
-                        const float w = 2.0f * vrz * vrx;
-                        tzx[(r - 8) * IW + c - 4] = make_float2(w * b.h1, w * b.h2);
-                    }
+                txy[(ty + 4) * IW + tx + 4] = mul2(f2(2.0f * g.y * g.z), H);
+                tyz[(ty + 4) * TX + tx] = mul2(f2(2.0f * g.z * g.w), H);
+                tzx[ty * IW + tx + 4] = mul2(f2(2.0f * g.w * g.y), H);
+            }
+        }
+        // rows above and below the core, columns 8..39: yy (rows 0..3, 28..31),
+        // yy + xy + yz (rows 4..7, 24..27); one row per warp
+        {
+            const bool inner = warp >= 8;  // rows 4..7, 24..27
+            const int w = warp & 7;
+            const int r = inner ? (w < 4 ? 4 + w : 20 + w) : (w < 4 ? w : 24 + w);
+            const int c = 8 + lane;
+            const int k = r * PW + c;
+            float2 S, H;
+            base(k, S, H);
+            const float4 g = geo(k);
+            tyy[r * TX + lane] = mul2(f2(rcp_approx(g.x)), fma2(f2(g.z * g.z), H, S));
+            if constexpr (TTI) {
+                if (inner) {
+                    txy[(r - 4) * IW + c - 4] = mul2(f2(2.0f * g.y * g.z), H);
+                    tyz[(r - 4) * TX + lane] = mul2(f2(2.0f * g.z * g.w), H);
                 }
             }
-        };
-        temps_at(ty, tx);
-        temps_at(ty + TY, tx);
-        // the (PW-TX) x PH right columns: one position per thread, whole warps
-        static_assert((PW - TX) * PH == NT, "right columns of the staging tile: one per thread");
-        temps_at(tid / (PW - TX), TX + tid % (PW - TX));
-        // this column's zz temporary and buoyancy at plane L
-        const int kc = (ty + 8) * PW + tx + 8;
-        float tz1, tz2;
-        {
-            const Base b = base_at(st, kc);
-            const float vr = TTI ? srz[(ty + 4) * IW + tx + 4] : 1.0f;
-            const float rr = vr * vr;
-            tz1 = b.rho * (b.s1 + rr * b.h1);
-            tz2 = b.rho * (b.s2 + rr * b.h2);
+        }
+        // columns left and right of the core, rows 8..23: xx (columns 0..3,
+        // 44..47; warps 0..3), xx + xy + zx (columns 4..7, 40..43; warps
+        // 4..7); the xy corners (rows 4..7, 24..27 x columns 4..7, 40..43;
+        // warps 8, 9)
+        if (warp < 8) {
+            const bool inner = warp >= 4;
+            const int r = 8 + 4 * (warp & 3) + (lane >> 3), cc = lane & 7;
+            const int c = inner ? (cc < 4 ? 4 + cc : 36 + cc) : (cc < 4 ? cc : 40 + cc);
+            const int k = r * PW + c;
+            float2 S, H;
+            base(k, S, H);
+            const float4 g = geo(k);
+            txx[(r - 8) * PW + c] = mul2(f2(rcp_approx(g.x)), fma2(f2(g.y * g.y), H, S));
+            if constexpr (TTI) {
+                if (inner) {
+                    txy[(r - 4) * IW + c - 4] = mul2(f2(2.0f * g.y * g.z), H);
+                    tzx[(r - 8) * IW + c - 4] = mul2(f2(2.0f * g.w * g.y), H);
+                }
+            }
+        } else if (TTI && warp < 10) {
+            const int i = (warp - 8) * 32 + lane, rr = i >> 3, cc = i & 7;
+            const int r = rr < 4 ? 4 + rr : 20 + rr, c = cc < 4 ? 4 + cc : 36 + cc;
+            const int k = r * PW + c;
+            float2 S, H;
+            base(k, S, H);
+            const float4 g = geo(k);
+            txy[(r - 4) * IW + c - 4] = mul2(f2(2.0f * g.y * g.z), H);
         }
 #pragma unroll
         for (int j = 0; j < 3; ++j) irq[j] = irq[j + 1];
-        irq[3] = st[S_IR * PH * PW + kc];
-        __syncthreads();  // temporaries of plane L are ready
+        irq[3] = irc;
+        if (__syncthreads_or(dead)) {  // temporaries of plane L are ready
+            stop = true;
+            break;
+        }
 
         // (2) buoyancy-scaled x/y derivatives of plane L (compute_xy_contributions)
         // dxs[r][c]: x = x0-4+c, y = y0+r;  dys[r][c]: x = x0+c, y = y0-4+r
-        auto dx_at = [&](int r, int c) {
+        auto dx_at = [&](int r, int c, float irv) {
             const bool in = (x0 - 4 + c >= L.ixbeg) && (x0 - 4 + c <= L.ixend);
-            const float irv = st[S_IR * PH * PW + (r + 8) * PW + c + 4];
             const float2* T = txx + r * PW + c + 4;
-            float acc1 = 0.0f, acc2 = 0.0f;
+            float2 acc = f2(0.0f);
 #pragma unroll
-            for (int i = 1; i <= 4; ++i) {
-                const float2 hi = T[i - 1], lo = T[-i];
-                acc1 += (a.invdx * c1(i)) * (hi.x - lo.x) * irv;
-                acc2 += (a.invdx * c1(i)) * (hi.y - lo.y) * irv;
-            }
-            dxs[r * IW + c] = in ? make_float2(acc1, acc2) : make_float2(0.0f, 0.0f);
+            for (int i = 1; i <= 4; ++i) acc = fma2(a.kd[0][i - 1], sub2(T[i - 1], T[-i]), acc);
+            dxs[r * IW + c] = in ? mul2(acc, f2(irv)) : f2(0.0f);
         };
-        auto dy_at = [&](int r, int c) {
+        auto dy_at = [&](int r, int c, float irv) {
             const bool in = (y0 - 4 + r >= L.iybeg) && (y0 - 4 + r <= L.iyend);
-            const float irv = st[S_IR * PH * PW + (r + 4) * PW + c + 8];
             const float2* T = tyy + (r + 4) * TX + c;
-            float acc1 = 0.0f, acc2 = 0.0f;
+            float2 acc = f2(0.0f);
 #pragma unroll
-            for (int i = 1; i <= 4; ++i) {
-                const float2 hi = T[(i - 1) * TX], lo = T[-i * TX];
-                acc1 += (a.invdy * c1(i)) * (hi.x - lo.x) * irv;
-                acc2 += (a.invdy * c1(i)) * (hi.y - lo.y) * irv;
-            }
-            dys[r * TX + c] = in ? make_float2(acc1, acc2) : make_float2(0.0f, 0.0f);
+            for (int i = 1; i <= 4; ++i) acc = fma2(a.kd[1][i - 1], sub2(T[(i - 1) * TX], T[-i * TX]), acc);
+            dys[r * TX + c] = in ? mul2(acc, f2(irv)) : f2(0.0f);
         };
-        dx_at(ty, tx);
-        if (tid < (IW - TX) * TY) dx_at(tid / (IW - TX), TX + tid % (IW - TX));
-        dy_at(ty, tx);
-        if (ty < IH - TY) dy_at(ty + TY, tx);
+        dx_at(ty, tx + 4, irc);
+        dy_at(ty + 4, tx, irc);
+        if (warp < 4) {  // x halo of dxs: columns 0..3, 36..39
+            const int i = warp * 32 + lane, r = i >> 3, cc = i & 7;
+            const int c = cc < 4 ? cc : 32 + cc;
+            dx_at(r, c, geo((r + 8) * PW + c + 4).x);
+        } else if (warp < 12) {  // y halo of dys: rows 0..3, 20..23
+            const int w = warp - 4;
+            const int r = w < 4 ? w : 16 + w;
+            dy_at(r, lane, geo((r + 4) * PW + lane + 8).x);
+        }
         // (3) D- z stage (compute_z_contributionsdtd), completes position L-3
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float alpha = (j <= 3) ? a.invdz * c1(4 - j) : -a.invdz * c1(j - 3);
-            dzq1[j] = dzq1[j] + alpha * tz1;
-            dzq2[j] = dzq2[j] + alpha * tz2;
-        }
+        for (int j = 0; j < 8; ++j) dzq[j] = fma2(a.kzm[j], tz, dzq[j]);
         {
             const int zp = Lz - 3;
             const bool valid = (zp >= L.izbeg + (a.fs ? 1 : 0)) && zp <= L.izend;
-            const float n1 = valid ? dzq1[0] * irq[0] : 0.0f;
-            const float n2 = valid ? dzq2[0] * irq[0] : 0.0f;
+            const float2 n = valid ? mul2(dzq[0], f2(irq[0])) : f2(0.0f);
 #pragma unroll
             for (int j = 0; j < 7; ++j) {
-                dZ1[j] = dZ1[j + 1];
-                dZ2[j] = dZ2[j + 1];
-                dzq1[j] = dzq1[j + 1];
-                dzq2[j] = dzq2[j + 1];
+                dZ[j] = dZ[j + 1];
+                dzq[j] = dzq[j + 1];
             }
-            dZ1[7] = n1;
-            dZ2[7] = n2;
-            dzq1[7] = 0.0f;
-            dzq2[7] = 0.0f;
+            dZ[7] = n;
+            dzq[7] = f2(0.0f);
         }
-        // (4) mixed rhs: scatter of plane L into outputs L-4 .. L+4, then xy into output L
+        // (4) yz/zx rhs: scatter of plane L into outputs L-4 .. L+4; output
+        //     L-4 is then complete and moves to the in-plane queue
+        float2 xy34 = f2(0.0f);
         if constexpr (TTI) {
+            // differences around this column, once per distance i: plane L
+            // adds c2(i)*(T[+i] - T[-i]) to output L-i and its negative to L+i
+            float2 dyz[4], dzx[4];
+#pragma unroll
+            for (int i = 1; i <= 4; ++i) {
+                dyz[i - 1] = sub2(tyz[(ty + 4 + i) * TX + tx], tyz[(ty + 4 - i) * TX + tx]);
+                dzx[i - 1] = sub2(tzx[ty * IW + tx + 4 + i], tzx[ty * IW + tx + 4 - i]);
+            }
+            float2 top = f2(0.0f);  // output L+4
 #pragma unroll
             for (int ir = -4; ir <= 4; ++ir) {
                 if (ir == 0) continue;
-                const float c = c2(ir < 0 ? -ir : ir);
-                const int j = 7 - ir;  // output L - ir
-                const float2 yp = tyz[(ty + 4 + ir) * TX + tx], ym = tyz[(ty + 4 - ir) * TX + tx];
-                const float2 zp = tzx[ty * IW + tx + 4 + ir], zm = tzx[ty * IW + tx + 4 - ir];
-                const float t1 = (a.invdyz * c) * (yp.x - ym.x);
-                const float t2 = (a.invdzx * c) * (zp.x - zm.x);
-                const float u1 = (a.invdyz * c) * (yp.y - ym.y);
-                const float u2 = (a.invdzx * c) * (zp.y - zm.y);
-                mx1[j] = mx1[j] + t1 + t2;
-                mx2[j] = mx2[j] + u1 + u2;
+                const int i = ir < 0 ? -ir : ir;
+                float2& o = (ir == -4) ? top : mq[4 - ir];  // output L - ir
+                o = fma2(a.kyz[ir + 4], dyz[i - 1], o);
+                o = fma2(a.kzx[ir + 4], dzx[i - 1], o);
             }
+            sxy[3] = add2(sxy[3], mq[0]);  // output L-4 is complete
+#pragma unroll
+            for (int j = 0; j < 7; ++j) mq[j] = mq[j + 1];
+            mq[7] = top;
+            // xy of output L from plane L
             const int cc = tx + 4, rr = ty + 4;
-            float s3 = mx1[7], s4 = mx2[7];
 #pragma unroll
             for (int k = 1; k <= 4; ++k) {
-                const float axy = a.invdxy * c2(k);
                 const float2 pp = txy[(rr + k) * IW + cc + k], pm = txy[(rr + k) * IW + cc - k];
                 const float2 mm = txy[(rr - k) * IW + cc - k], mp = txy[(rr - k) * IW + cc + k];
-                s3 += axy * (pp.x - pm.x + mm.x - mp.x);
-                s4 += axy * (pp.y - pm.y + mm.y - mp.y);
+                xy34 = fma2(a.kxy[k - 1], sub2(add2(sub2(pp, pm), mm), mp), xy34);
             }
-            mx1[7] = s3;
-            mx2[7] = s4;
         }
         __syncthreads();  // dxs/dys of plane L are ready
 
         // (5) x+y parts of output L (dfdx_stg_right, kernel_type2_adj.cu:85-98)
         {
-            float sx1 = 0, sx2 = 0, sy1 = 0, sy2 = 0;
+            float2 acc = xy34;
 #pragma unroll
             for (int k = 1; k <= 4; ++k) {
-                const float2 xp = dxs[ty * IW + tx + 4 + k], xm = dxs[ty * IW + tx + 5 - k];
-                const float2 yp = dys[(ty + 4 + k) * TX + tx], ym = dys[(ty + 5 - k) * TX + tx];
-                sx1 += c1(k) * (xp.x - xm.x);
-                sx2 += c1(k) * (xp.y - xm.y);
-                sy1 += c1(k) * (yp.x - ym.x);
-                sy2 += c1(k) * (yp.y - ym.y);
+                acc = fma2(a.kd[0][k - 1], sub2(dxs[ty * IW + tx + 4 + k], dxs[ty * IW + tx + 5 - k]), acc);
+                acc = fma2(a.kd[1][k - 1], sub2(dys[(ty + 4 + k) * TX + tx], dys[(ty + 5 - k) * TX + tx]), acc);
             }
-            sx1 *= a.invdx;
-            sx2 *= a.invdx;
-            sy1 *= a.invdy;
-            sy2 *= a.invdy;
-            sxy1[7] = sx1 + sy1;
-            sxy2[7] = sx2 + sy2;
+            sxy[7] = acc;
         }
         // (6) output plane L-7
         const int z = zo;
         if (out_here) {
             const int64_t gi = go;
-            float q1[8], q2[8];
+            float2 q[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                q1[j] = dZ1[j];
-                q2[j] = dZ2[j];
-            }
-            if (a.fs) {
-                resolve_dz(q1, z - L.izbeg);
-                resolve_dz(q2, z - L.izbeg);
-            }
-            float sz1 = 0, sz2 = 0;
+            for (int j = 0; j < 8; ++j) q[j] = dZ[j];
+            if (a.fs) resolve_dz(q, z - L.izbeg);
+            float2 r34 = sxy[0];
 #pragma unroll
-            for (int k = 1; k <= 4; ++k) {
-                sz1 += c1(k) * (q1[3 + k] - q1[4 - k]);
-                sz2 += c1(k) * (q2[3 + k] - q2[4 - k]);
-            }
-            sz1 *= a.invdz;
-            sz2 *= a.invdz;
-            float r3 = sxy1[0] + sz1;
-            float r4 = sxy2[0] + sz2;
-            r3 += mx1[0];
-            r4 += mx2[0];
+            for (int k = 1; k <= 4; ++k) r34 = fma2(a.kd[2][k - 1], sub2(q[3 + k], q[4 - k]), r34);
             const float2 sz = osz;
-            float n3, n4;
+            float2 n34;
             if (a.sponge) {
                 const float A = fminf(fminf(sx.x, sy.x), sz.x);
                 const float B = fminf(fminf(sx.y, sy.y), sz.y) * a.dt;
-                n3 = A * o3 + B * r3;
-                n4 = A * o4 + B * r4;
+                n34 = fma2(f2(B), r34, mul2(f2(A), o34));
             } else {
-                n3 = o3 + r3 * a.dt;
-                n4 = o4 + r4 * a.dt;
+                n34 = fma2(r34, f2(a.dt), o34);
             }
-            a.f3[gi] = n3;
-            a.f4[gi] = n4;
+            a.f3[gi] = n34.x;
+            a.f4[gi] = n34.y;
             // loop2 (kernel_base.cu:92-101) and free surface (:142-162)
             const float A = fminf(sx.x, fminf(sy.x, sz.x));
             const float B = fminf(sx.y, fminf(sy.y, sz.y));
-            float np = A * opc + B * n3 * a.dt;
-            float nq = A * oqc + B * n4 * a.dt;
-            if (a.fs && z == L.izbeg) {
-                np = 0.0f;
-                nq = 0.0f;
-            }
-            wave_apply(a.wave_prec, a.wave_scale, np, nq);
-            a.pout[gi] = np;
-            a.qout[gi] = nq;
+            float2 npq = fma2(mul2(f2(B), n34), f2(a.dt), mul2(f2(A), opq));
+            if (a.fs && z == L.izbeg) npq = f2(0.0f);
+            wave_apply(a.wave_prec, a.wave_scale, npq.x, npq.y);
+            a.pout[gi] = npq.x;
+            a.qout[gi] = npq.y;
             if (a.fs && z > L.izbeg && z <= L.izbeg + kRadius) {
                 const int64_t gm = L.idx(x, y, 2 * L.izbeg - z);
-                a.pout[gm] = -np;
-                a.qout[gm] = -nq;
+                a.pout[gm] = -npq.x;
+                a.qout[gm] = -npq.y;
             }
         }
-        // (7) rotate the output queues
+        // (7) rotate the in-plane queue
 #pragma unroll
-        for (int j = 0; j < 7; ++j) {
-            sxy1[j] = sxy1[j + 1];
-            sxy2[j] = sxy2[j + 1];
-        }
-#pragma unroll
-        for (int j = 0; j < 11; ++j) {
-            mx1[j] = mx1[j + 1];
-            mx2[j] = mx2[j + 1];
-        }
-        mx1[11] = 0.0f;
-        mx2[11] = 0.0f;
+        for (int j = 0; j < 7; ++j) sxy[j] = sxy[j + 1];
         if (++s == ADJ_NSTAGE) {
             s = 0;
             phase ^= 1u;
         }
     }
+    if (stop) break;
     }  // segments
+    if (stop && tid == 0) drain_loads(bars, ADJ_NSTAGE, g_wait, g_issued);
 }
 
 // ---------------------------------------------------------------------------
@@ -970,7 +1039,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
 // interior volumes, free-surface halo re-derived by mirroring); the adjoint
 // temporaries adj_a = rho*(s1 + ra^2 h1) come from the current adjoint p/q.
 struct ImgParams {
-    const float *f3, *f4, *rz, *irho;
+    const float *f3, *f4;
     const void *snap3, *snap4;  // dense pdot/qdot of this snapshot (storage type)
     const float* snap_scale;    // the 4 multipliers the slot was stored with
     float *gvp, *grho;           // dense images
@@ -981,56 +1050,44 @@ struct ImgParams {
     int slot;                    // snapshot index in the store
     float hx, hy, hz;
     int* err;
+    // stg_d1 coefficients with the grid spacings folded in, as (c, c) pairs
+    float2 kcx[4], kcy[4], kcz[4];  // cs(r)/dx, /dy, /dz
+    float2 kcxn[4], kcyn[4];        // -cs(r)/dx, -cs(r)/dy
 };
 
 constexpr int IMG_NSTAGE = 3;
 constexpr int IMG_PF = 2;
-constexpr int IMG_NADJ = 9;  // f1, f2, m1, m2, m3, m4, irho, rx, ry with a halo of 4
+// Staging per plane: the stored p, q (storage type, halo 8), then the
+// adjoint p, q (float) and the interleaved model (m1, m2, m3, m4) and
+// (irho, rx, ry, rz) (float4; VTI: irho as float), halo 4.
 __host__ __device__ constexpr size_t img_p(size_t elt) { return (size_t)PH * PW * elt; }
 constexpr size_t IMG_A = (size_t)IH * IW * sizeof(float);
-__host__ __device__ constexpr size_t img_stage(size_t elt) { return 2 * img_p(elt) + IMG_NADJ * IMG_A; }
+constexpr size_t IMG_A4 = (size_t)IH * IW * sizeof(float4);
+__host__ __device__ constexpr size_t img_stage(size_t elt, bool tti)
+{
+    return 2 * img_p(elt) + 2 * IMG_A + IMG_A4 + (tti ? IMG_A4 : IMG_A);
+}
 constexpr size_t IMG_T1 = (size_t)2 * TY * IW * sizeof(float);  // x-type tiles: rows y0.., cols x0-4..
 constexpr size_t IMG_T2 = (size_t)2 * IH * TX * sizeof(float);  // y-type tiles: rows y0-4.., cols x0..
-__host__ __device__ constexpr size_t img_smem(size_t elt)
+__host__ __device__ constexpr size_t img_smem(size_t elt, bool tti)
 {
-    return IMG_NSTAGE * img_stage(elt) + 2 * IMG_T1 + 2 * IMG_T2 + IMG_NSTAGE * sizeof(uint64_t);
+    return IMG_NSTAGE * img_stage(elt, tti) + 2 * IMG_T1 + 2 * IMG_T2 + IMG_NSTAGE * sizeof(uint64_t);
 }
 
 struct ImgMaps {
-    CUtensorMap snap;            // 4D over the store: (nx, ny, nz, 4*nsnap), box PW x PH
-    CUtensorMap a[IMG_NADJ];     // box IW x IH over halo'd volumes
+    CUtensorMap snap;   // 4D over the store: (nx, ny, nz, 4*nsnap), box PW x PH
+    CUtensorMap p, q;   // adjoint p, q: box IW x IH
+    CUtensorMap ma;     // 4D (4, x, y, z), box 4 x IW x IH
+    CUtensorMap mb;     // TTI: like ma; VTI: irho, box IW x IH
 };
-enum { A_P = 0, A_Q, A_M1, A_M2, A_M3, A_M4, A_IR, A_RX, A_RY };
 
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
-                                            uint64_t* bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];" ::"r"(saddr(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(saddr(bar))
-        : "memory");
-}
-
-// adjoint temporary rho*(s1 + r^2 h1), rho*(s2 + r^2 h2) at staging offset k (halo-4 tile)
-__device__ __forceinline__ float2 img_adj(const float* A, int k, float ra)
-{
-    const float p = A[A_P * IH * IW + k], q = A[A_Q * IH * IW + k];
-    const float a1 = A[A_M1 * IH * IW + k], a2 = A[A_M2 * IH * IW + k], a3 = A[A_M3 * IH * IW + k],
-                a4 = A[A_M4 * IH * IW + k];
-    const float rho = __frcp_rn(A[A_IR * IH * IW + k]);
-    const float rr = ra * ra;
-    const float lx = (a4 - a1) * p - a2 * q;
-    const float lz = a2 * p + (a3 - a4) * q;
-    return make_float2(rho * (a1 * p + a2 * q + rr * lx), rho * (a4 * q + rr * lz));
-}
 
 template <bool TTI, typename T>
 __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ ImgMaps tm, const ImgParams a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     constexpr size_t IMG_P = img_p(sizeof(T));
-    constexpr size_t IMG_STAGE = img_stage(sizeof(T));
+    constexpr size_t IMG_STAGE = img_stage(sizeof(T), TTI);
     unsigned char* stage = smem;
     unsigned char* sp = smem + IMG_NSTAGE * IMG_STAGE;
     // x-type and y-type tiles, one float4 per cell: forward derivative of
@@ -1046,8 +1103,9 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int nx = L.nx(), ny = L.ny();
     bool dead = false;
-    constexpr int NADJ = TTI ? IMG_NADJ : A_RX;
-    constexpr uint32_t TX_BYTES = (uint32_t)(2 * IMG_P + NADJ * IMG_A);
+    bool stop = false;             // the CTA gave up (a bounded wait timed out)
+    int g_issued = 0, g_wait = 0;  // planes issued (thread 0) / plane last waited on
+    constexpr uint32_t TX_BYTES = (uint32_t)IMG_STAGE;
     // stored values are value*scale with a power-of-two scale: undo exactly
     float us1 = 1.0f, us2 = 1.0f, us3 = 1.0f, us4 = 1.0f;
     if (a.snap_scale) {
@@ -1056,6 +1114,10 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
         us1 = 1.0f / a.snap_scale[2];
         us2 = 1.0f / a.snap_scale[3];
     }
+    // unscaling of the stored p, q folded into the derivative scales (exact:
+    // powers of two)
+    const float2 ux = make_float2(us1 * a.hx, us2 * a.hx), uy = make_float2(us1 * a.hy, us2 * a.hy);
+    const float2 uz = make_float2(us1 * a.hz, us2 * a.hz), u12 = make_float2(us1, us2);
 
     if (tid == 0) {
         for (int s = 0; s < IMG_NSTAGE; ++s) mbar_init(&bars[s], 1);
@@ -1072,11 +1134,15 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
     const int ntot = sg.len + 2 * LAG;
     const int x = x0 + tx, y = y0 + ty;
     const bool owner = (x <= L.ixend) && (y <= L.iyend);
-    __syncthreads();  // barriers initialised; the previous segment is done with the stages
+    if (__syncthreads_or(dead)) {  // barriers initialised; the previous segment is done with the stages
+        stop = true;
+        break;
+    }
 
     // plane z of the stored p/q: dense z = z - izbeg; above the surface the
     // free surface mirrors it (2*izbeg - z), without one it is zero halo.
     auto issue = [&](int t) {
+        ++g_issued;
         const int s = (gbase + t) % IMG_NSTAGE, z = zs - LAG + t;
         unsigned char* dst = stage + (size_t)s * IMG_STAGE;
         mbar_expect_tx(&bars[s], TX_BYTES);
@@ -1084,25 +1150,37 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
         if (a.fs && zd < 0) zd = -zd;
         tma_load_4d(dst, &tm.snap, xd0 - 8, yd0 - 8, zd, 4 * a.slot + 2, &bars[s]);
         tma_load_4d(dst + IMG_P, &tm.snap, xd0 - 8, yd0 - 8, zd, 4 * a.slot + 3, &bars[s]);
-        float* adst = reinterpret_cast<float*>(dst + 2 * IMG_P);
-#pragma unroll
-        for (int k = 0; k < NADJ; ++k) tma_load_3d(adst + k * IH * IW, &tm.a[k], x0 - 4, y0 - 4, z, &bars[s]);
+        unsigned char* adst = dst + 2 * IMG_P;
+        tma_load_3d(adst, &tm.p, x0 - 4, y0 - 4, z, &bars[s]);
+        tma_load_3d(adst + IMG_A, &tm.q, x0 - 4, y0 - 4, z, &bars[s]);
+        tma_load_4d(adst + 2 * IMG_A, &tm.ma, 0, x0 - 4, y0 - 4, z, &bars[s]);
+        if constexpr (TTI)
+            tma_load_4d(adst + 2 * IMG_A + IMG_A4, &tm.mb, 0, x0 - 4, y0 - 4, z, &bars[s]);
+        else
+            tma_load_3d(adst + 2 * IMG_A + IMG_A4, &tm.mb, x0 - 4, y0 - 4, z, &bars[s]);
     };
     if (tid == 0)
         for (int t = 0; t < IMG_PF && t < ntot; ++t) issue(t);
 
-    float dzq1[8], dzq2[8];  // D- partial sums of the stored p/q, positions L-3 .. L+4
-    float fz1[8], fz2[8];    // forward z derivatives, positions L-10 .. L-3
-    float az1q[12], az2q[12];  // adjoint z temporaries, planes L-11 .. L
-    float rxy[8];            // x+y part of the gradient rhs, outputs L-7 .. L
-    float irq[8];            // buoyancy of this column, planes L-7 .. L
+    // register queues, both fields of a cell in one pair
+    float2 dzq[8];   // D- partial sums of the stored p/q, positions L-3 .. L+4
+    float2 fz[8];    // forward z derivatives, positions L-10 .. L-3
+    float2 azq[12];  // adjoint z temporaries, planes L-11 .. L
+    float rxy[8];    // x+y part of the gradient rhs, outputs L-7 .. L
+    float irq[8];    // buoyancy of this column, planes L-7 .. L
 #pragma unroll
-    for (int j = 0; j < 8; ++j) dzq1[j] = dzq2[j] = fz1[j] = fz2[j] = rxy[j] = irq[j] = 0.0f;
+    for (int j = 0; j < 8; ++j) {
+        dzq[j] = fz[j] = f2(0.0f);
+        rxy[j] = irq[j] = 0.0f;
+    }
 #pragma unroll
-    for (int j = 0; j < 12; ++j) az1q[j] = az2q[j] = 0.0f;
+    for (int j = 0; j < 12; ++j) azq[j] = f2(0.0f);
 
     for (int t = 0; t < ntot; ++t) {
-        __syncthreads();  // the x/y tiles of plane L-1 have been read by every thread
+        if (__syncthreads_or(dead)) {  // the x/y tiles of plane L-1 have been read by every thread
+            stop = true;
+            break;
+        }
         if (tid == 0 && t + IMG_PF < ntot) {
             fence_proxy_async();
             issue(t + IMG_PF);
@@ -1123,8 +1201,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             pgv = a.gvp[dvp];
         }
         if (rho_here) pgr = a.grho[drho];
-        const int64_t gcol = L.idx(min(x, L.ldimx - 1), min(y, L.ldimy - 1), min(max(Lz, 0), L.ldimz - 1));
-        const float prz = TTI ? __ldg(a.rz + gcol) : 1.0f;
+        g_wait = gbase + t;
         mbar_wait(&bars[s], phase, a.err, dead);
         unsigned char* st = stage + (size_t)s * IMG_STAGE;
         const bool mirrored = a.fs && Lz < L.izbeg;
@@ -1135,48 +1212,55 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
         }
         const T* P1 = reinterpret_cast<const T*>(st);
         const T* P2 = P1 + PH * PW;
-        const float* A = reinterpret_cast<const float*>(st + 2 * IMG_P);
+        const float* AP = reinterpret_cast<const float*>(st + 2 * IMG_P);
+        const float* AQ = AP + IH * IW;
+        const float4* AMA = reinterpret_cast<const float4*>(st + 2 * IMG_P + 2 * IMG_A);
+        const float4* AMB = AMA + IH * IW;                                // TTI
+        const float* AIR = reinterpret_cast<const float*>(AMA + IH * IW);  // VTI
+        // (irho, rx, ry, rz) at offset k of the halo-4 tiles
+        auto geo = [&](int k) {
+            if constexpr (TTI) return AMB[k];
+            else return make_float4(AIR[k], 0.0f, 0.0f, 1.0f);
+        };
+        // adjoint temporary rho*(S + r^2 H) at offset k (kernel_type2_grad.cu:
+        // 435-439), S = (m1 p + m2 q, m4 q), H = ((m4 - m1) p - m2 q, m2 p + (m3 - m4) q)
+        auto adj_t = [&](int k, float irho, float ra) {
+            const float p = AP[k], q = AQ[k];
+            const float4 m = AMA[k];
+            const float2 S = fma2(make_float2(m.y, m.w), f2(q), make_float2(m.x * p, 0.0f));
+            const float2 H = fma2(make_float2(m.w - m.x, m.z - m.w), make_float2(p, q), make_float2(-(m.y * q), m.y * p));
+            return mul2(f2(rcp_approx(irho)), fma2(f2(ra * ra), H, S));
+        };
         const int kc = (ty + 4) * IW + tx + 4;  // this column in a halo-4 tile
+        // the stored (p, q) pair at offset k of the halo-8 tiles
+        auto spq = [&](int k) { return make_float2(to_f32(P1[k]), to_f32(P2[k])); };
 
         // (1) forward x/y derivatives of the stored p/q (fwd_drv) and the
         //     adjoint x/y temporaries of plane L.
         //     x-type tiles [r][c]: x = x0-4+c, y = y0+r; y-type: x = x0+c, y = y0-4+r
         auto xt_at = [&](int r, int c) {
             const bool in = (x0 - 4 + c >= L.ixbeg) && (x0 - 4 + c <= L.ixend);
-            const float irv = A[A_IR * IH * IW + (r + 4) * IW + c];
-            float acc[2];
-#pragma unroll
-            for (int f = 0; f < 2; ++f) {
-                const T* Pr = (f ? P2 : P1) + (r + 8) * PW + c + 4;
-                const float us = f ? us2 : us1;
-                acc[f] = 0.0f;
-#pragma unroll
-                for (int i = 1; i <= 4; ++i) acc[f] += c1(i) * (to_f32(Pr[i - 1]) * us - to_f32(Pr[-i]) * us);
-                acc[f] *= a.hx;
-                acc[f] = in ? acc[f] * irv : 0.0f;
-            }
             const int k = (r + 4) * IW + c;
-            const float2 t2 = img_adj(A, k, TTI ? A[A_RX * IH * IW + k] : 0.0f);
-            xs[r * IW + c] = make_float4(acc[0], acc[1], t2.x, t2.y);
+            const float4 g = geo(k);
+            const int k0 = (r + 8) * PW + c + 4;
+            float2 acc = f2(0.0f);
+#pragma unroll
+            for (int i = 1; i <= 4; ++i) acc = fma2(f2(c1(i)), sub2(spq(k0 + i - 1), spq(k0 - i)), acc);
+            acc = in ? mul2(mul2(acc, ux), f2(g.x)) : f2(0.0f);
+            const float2 t2 = adj_t(k, g.x, g.y);
+            xs[r * IW + c] = make_float4(acc.x, acc.y, t2.x, t2.y);
         };
         auto yt_at = [&](int r, int c) {
             const bool in = (y0 - 4 + r >= L.iybeg) && (y0 - 4 + r <= L.iyend);
-            const float irv = A[A_IR * IH * IW + r * IW + c + 4];
-            float acc[2];
-#pragma unroll
-            for (int f = 0; f < 2; ++f) {
-                const T* Pc = (f ? P2 : P1) + (r + 4) * PW + c + 8;
-                const float us = f ? us2 : us1;
-                acc[f] = 0.0f;
-#pragma unroll
-                for (int i = 1; i <= 4; ++i)
-                    acc[f] += c1(i) * (to_f32(Pc[(i - 1) * PW]) * us - to_f32(Pc[-i * PW]) * us);
-                acc[f] *= a.hy;
-                acc[f] = in ? acc[f] * irv : 0.0f;
-            }
             const int k = r * IW + c + 4;
-            const float2 t2 = img_adj(A, k, TTI ? A[A_RY * IH * IW + k] : 0.0f);
-            ys[r * TX + c] = make_float4(acc[0], acc[1], t2.x, t2.y);
+            const float4 g = geo(k);
+            const int k0 = (r + 4) * PW + c + 8;
+            float2 acc = f2(0.0f);
+#pragma unroll
+            for (int i = 1; i <= 4; ++i) acc = fma2(f2(c1(i)), sub2(spq(k0 + (i - 1) * PW), spq(k0 - i * PW)), acc);
+            acc = in ? mul2(mul2(acc, uy), f2(g.x)) : f2(0.0f);
+            const float2 t2 = adj_t(k, g.x, g.z);
+            ys[r * TX + c] = make_float4(acc.x, acc.y, t2.x, t2.y);
         };
         xt_at(ty, tx);
         if (tid < (IW - TX) * TY) xt_at(tid / (IW - TX), TX + tid % (IW - TX));
@@ -1184,43 +1268,33 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
         if (ty < IH - TY) yt_at(ty + TY, tx);
         // (2) column values: z temporaries, buoyancy, D- z stage of the stored p/q
         {
-            const float2 t2 = img_adj(A, kc, prz);
+            const float4 g = geo(kc);
+            const float2 t2 = adj_t(kc, g.x, g.w);
 #pragma unroll
-            for (int j = 0; j < 11; ++j) {
-                az1q[j] = az1q[j + 1];
-                az2q[j] = az2q[j + 1];
-            }
-            az1q[11] = t2.x;
-            az2q[11] = t2.y;
+            for (int j = 0; j < 11; ++j) azq[j] = azq[j + 1];
+            azq[11] = t2;
 #pragma unroll
             for (int j = 0; j < 7; ++j) irq[j] = irq[j + 1];
-            irq[7] = A[A_IR * IH * IW + kc];
-            const float v1 = to_f32(P1[(ty + 8) * PW + tx + 8]) * us1;
-            const float v2 = to_f32(P2[(ty + 8) * PW + tx + 8]) * us2;
+            irq[7] = g.x;
+            const float2 v = spq((ty + 8) * PW + tx + 8);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const float cf = dminus_coef(j);
-                dzq1[j] = dzq1[j] + cf * v1;
-                dzq2[j] = dzq2[j] + cf * v2;
-            }
+            for (int j = 0; j < 8; ++j) dzq[j] = fma2(f2(dminus_coef(j)), v, dzq[j]);
             const int zp = Lz - 3;
             const bool valid = (zp >= L.izbeg + (a.fs ? 1 : 0)) && zp <= L.izend;
             const float ir3 = irq[4];  // plane L-3
-            const float n1 = valid ? (dzq1[0] * a.hz) * ir3 : 0.0f;
-            const float n2 = valid ? (dzq2[0] * a.hz) * ir3 : 0.0f;
+            const float2 n = valid ? mul2(mul2(dzq[0], uz), f2(ir3)) : f2(0.0f);
 #pragma unroll
             for (int j = 0; j < 7; ++j) {
-                fz1[j] = fz1[j + 1];
-                fz2[j] = fz2[j + 1];
-                dzq1[j] = dzq1[j + 1];
-                dzq2[j] = dzq2[j + 1];
+                fz[j] = fz[j + 1];
+                dzq[j] = dzq[j + 1];
             }
-            fz1[7] = n1;
-            fz2[7] = n2;
-            dzq1[7] = 0.0f;
-            dzq2[7] = 0.0f;
+            fz[7] = n;
+            dzq[7] = f2(0.0f);
         }
-        __syncthreads();  // x/y tiles of plane L ready; staging slot s fully consumed
+        if (__syncthreads_or(dead)) {  // x/y tiles of plane L ready; staging slot s fully consumed
+            stop = true;
+            break;
+        }
 
         // (3) x+y part of the gradient rhs at plane L (compute_xy_contributions
         //     of kernel_type2_grad.cu:314-342 and :435-439) and the Vp image
@@ -1230,83 +1304,60 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             // positions -4 .. +4 around the cell, one 128-bit load each, folded
             // into the staggered sums as they arrive (D+ of the forward
             // derivatives uses -3..+4, D- of the adjoint temporaries -4..+3)
-            float dfx1 = 0, dfx2 = 0, dfy1 = 0, dfy2 = 0, dax1 = 0, dax2 = 0, day1 = 0, day2 = 0;
+            float2 dfx = f2(0.0f), dfy = f2(0.0f), dax = f2(0.0f), day = f2(0.0f);
             float4 xc, yc;
 #pragma unroll
             for (int j = 0; j < 9; ++j) {
                 const float4 u = xs[cx - 4 + j], w = ys[cy + (j - 4) * TX];
+                const float2 uf = make_float2(u.x, u.y), ua = make_float2(u.z, u.w);
+                const float2 wf = make_float2(w.x, w.y), wa = make_float2(w.z, w.w);
                 if (j >= 5) {
-                    dfx1 += cs(j - 5) * u.x;
-                    dfx2 += cs(j - 5) * u.y;
-                    dfy1 += cs(j - 5) * w.x;
-                    dfy2 += cs(j - 5) * w.y;
+                    dfx = fma2(a.kcx[j - 5], uf, dfx);
+                    dfy = fma2(a.kcy[j - 5], wf, dfy);
                 }
                 if (j >= 1 && j <= 4) {
-                    dfx1 -= cs(4 - j) * u.x;
-                    dfx2 -= cs(4 - j) * u.y;
-                    dfy1 -= cs(4 - j) * w.x;
-                    dfy2 -= cs(4 - j) * w.y;
+                    dfx = fma2(a.kcxn[4 - j], uf, dfx);
+                    dfy = fma2(a.kcyn[4 - j], wf, dfy);
                 }
                 if (j >= 4 && j <= 7) {
-                    dax1 += cs(j - 4) * u.z;
-                    dax2 += cs(j - 4) * u.w;
-                    day1 += cs(j - 4) * w.z;
-                    day2 += cs(j - 4) * w.w;
+                    dax = fma2(a.kcx[j - 4], ua, dax);
+                    day = fma2(a.kcy[j - 4], wa, day);
                 }
                 if (j <= 3) {
-                    dax1 -= cs(3 - j) * u.z;
-                    dax2 -= cs(3 - j) * u.w;
-                    day1 -= cs(3 - j) * w.z;
-                    day2 -= cs(3 - j) * w.w;
+                    dax = fma2(a.kcxn[3 - j], ua, dax);
+                    day = fma2(a.kcyn[3 - j], wa, day);
                 }
                 if (j == 4) {
                     xc = u;
                     yc = w;
                 }
             }
-            dfx1 *= a.hx;
-            dfx2 *= a.hx;
-            dfy1 *= a.hy;
-            dfy2 *= a.hy;
-            dax1 *= a.hx;
-            dax2 *= a.hx;
-            day1 *= a.hy;
-            day2 *= a.hy;
-            const float v = xc.z * dfx1 + xc.w * dfx2 + yc.z * dfy1 + yc.w * dfy2 + dax1 * xc.x + dax2 * xc.y +
-                            day1 * yc.x + day2 * yc.y;
+            float2 v2 = mul2(make_float2(xc.z, xc.w), dfx);
+            v2 = fma2(make_float2(yc.z, yc.w), dfy, v2);
+            v2 = fma2(dax, make_float2(xc.x, xc.y), v2);
+            v2 = fma2(day, make_float2(yc.x, yc.y), v2);
 #pragma unroll
             for (int j = 0; j < 7; ++j) rxy[j] = rxy[j + 1];
-            rxy[7] = v;
+            rxy[7] = v2.x + v2.y;
             if (vp_here) a.gvp[dvp] = pgv + (pa3 * ps3 + pa4 * ps4);
         }
         // (4) output plane L-7: z terms and the density gradient
         const int z = Lz - LAG;
         if (rho_here) {
-            float q1[8], q2[8];
+            float2 q[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                q1[j] = fz1[j];
-                q2[j] = fz2[j];
-            }
-            if (a.fs) {
-                resolve_dz(q1, z - L.izbeg);
-                resolve_dz(q2, z - L.izbeg);
-            }
-            // q[j] is position z-3+j; az*q[j] is plane z-4+j
-            float dfz1 = 0, dfz2 = 0, daz1 = 0, daz2 = 0;
+            for (int j = 0; j < 8; ++j) q[j] = fz[j];
+            if (a.fs) resolve_dz(q, z - L.izbeg);
+            // q[j] is position z-3+j; azq[j] is plane z-4+j
+            float2 dfz = f2(0.0f), daz = f2(0.0f);
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                const float c = cs(r);
-                dfz1 += c * (q1[4 + r] - q1[3 - r]);
-                dfz2 += c * (q2[4 + r] - q2[3 - r]);
-                daz1 += c * (az1q[4 + r] - az1q[3 - r]);
-                daz2 += c * (az2q[4 + r] - az2q[3 - r]);
+                dfz = fma2(a.kcz[r], sub2(q[4 + r], q[3 - r]), dfz);
+                daz = fma2(a.kcz[r], sub2(azq[4 + r], azq[3 - r]), daz);
             }
-            dfz1 *= a.hz;
-            dfz2 *= a.hz;
-            daz1 *= a.hz;
-            daz2 *= a.hz;
-            const float rhs = rxy[0] + az1q[4] * dfz1 + az2q[4] * dfz2 + daz1 * q1[3] + daz2 * q2[3];
+            float2 r2 = mul2(azq[4], dfz);
+            r2 = fma2(daz, q[3], r2);
+            const float rhs = rxy[0] + (r2.x + r2.y);
             a.grho[drho] = pgr + -irq[0] * rhs;
         }
         if (++s == IMG_NSTAGE) {
@@ -1314,7 +1365,9 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             phase ^= 1u;
         }
     }
+    if (stop) break;
     }  // segments
+    if (stop && tid == 0) drain_loads(bars, IMG_NSTAGE, g_wait, g_issued);
 }
 
 // ---------------------------------------------------------------------------
@@ -1490,6 +1543,8 @@ __global__ void __launch_bounds__(T1X2_NT, 2)
     const Layout& L = a.L;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * T1X2_TX + tx;
     bool dead = false;
+    bool stop = false;                   // the CTA gave up (a bounded wait timed out)
+    int g_issued = 0, g_wait = 0;  // planes issued (thread 0) / plane last waited on
     if (tid == 0) {
         for (int s = 0; s < T1_NS; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
@@ -1505,8 +1560,12 @@ __global__ void __launch_bounds__(T1X2_NT, 2)
         const int xa = x0 + 2 * tx, y = y0 + ty;
         const bool own_a = (xa <= L.ixend) && (y <= L.iyend);
         const bool own_b = own_a && (xa + 1 <= L.ixend);
-        __syncthreads();
+        if (__syncthreads_or(dead)) {
+            stop = true;
+            break;
+        }
         auto issue = [&](int t) {
+            ++g_issued;
             const int sl = (gbase + t) % T1_NS, z = zs - T1_LAG + t;
             float* dst = ring + (size_t)sl * 2 * IH * IW;
             mbar_expect_tx(&bars[sl], (uint32_t)T1_SLOT);
@@ -1518,11 +1577,15 @@ __global__ void __launch_bounds__(T1X2_NT, 2)
         const int vc = 2 * tx + 4, vr = ty + 4;
         auto back = [&](int kk) { const int v = s - kk; return v < 0 ? v + T1_NS : v; };
         for (int t = 0; t < ntot; ++t) {
-            __syncthreads();  // every thread is done with iteration t-1
+            if (__syncthreads_or(dead)) {  // every thread is done with iteration t-1
+                stop = true;
+                break;
+            }
             if (tid == 0 && t + T1_PF < ntot) {
                 fence_proxy_async();
                 issue(t + T1_PF);
             }
+            g_wait = gbase + t;
             mbar_wait(&bars[s], phase, a.err, dead);
             const int z = zs - T1_LAG + t - T1_LAG;  // output plane
             float snapv[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
@@ -1622,7 +1685,9 @@ __global__ void __launch_bounds__(T1X2_NT, 2)
                 phase ^= 1u;
             }
         }
+    if (stop) break;
     }  // segments
+    if (stop && tid == 0) drain_loads(bars, T1_NS, g_wait, g_issued);
     if (a.snap && a.snap_prec != SNAP_F32) {
 #pragma unroll
         for (int f = 0; f < 2; ++f) {
@@ -1693,6 +1758,8 @@ __global__ void __launch_bounds__(NT, 1) k_t1_fused_adjoint(const __grid_constan
     const Layout& L = a.L;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     bool dead = false;
+    bool stop = false;                   // the CTA gave up (a bounded wait timed out)
+    int g_issued = 0, g_wait = 0;  // planes issued (thread 0) / plane last waited on
     constexpr int NLOAD = TTI ? T1A_NARR : U_RX;
     constexpr uint32_t TX_BYTES = (uint32_t)(NLOAD * IH * IW * sizeof(float));
     if (tid == 0) {
@@ -1708,8 +1775,12 @@ __global__ void __launch_bounds__(NT, 1) k_t1_fused_adjoint(const __grid_constan
         const int ntot = sg.len + 2 * T1_LAG;
         const int x = x0 + tx, y = y0 + ty;
         const bool owner = (x <= L.ixend) && (y <= L.iyend);
-        __syncthreads();
+        if (__syncthreads_or(dead)) {
+            stop = true;
+            break;
+        }
         auto issue = [&](int t) {
+            ++g_issued;
             const int sl = (gbase + t) % T1A_NSTAGE, z = zs - T1_LAG + t;
             float* dst = stage + (size_t)sl * (T1A_STAGE / sizeof(float));
             mbar_expect_tx(&bars[sl], TX_BYTES);
@@ -1722,7 +1793,10 @@ __global__ void __launch_bounds__(NT, 1) k_t1_fused_adjoint(const __grid_constan
 #pragma unroll
         for (int j = 0; j < 9; ++j) q3[j] = q4[j] = 0.0f;
         for (int t = 0; t < ntot; ++t) {
-            __syncthreads();  // the tiles of plane L-1 have been read; stage (t+2)%3 is free
+            if (__syncthreads_or(dead)) {  // the tiles of plane L-1 have been read; stage (t+2)%3 is free
+                stop = true;
+                break;
+            }
             if (tid == 0 && t + T1A_PF < ntot) {
                 fence_proxy_async();
                 issue(t + T1A_PF);
@@ -1742,6 +1816,7 @@ __global__ void __launch_bounds__(NT, 1) k_t1_fused_adjoint(const __grid_constan
                 osy = __ldg(a.aby + y);
                 osz = __ldg(a.abz + zo);
             }
+            g_wait = gbase + t;
             mbar_wait(&bars[s], phase, a.err, dead);
             const float* st = stage + (size_t)s * (T1A_STAGE / sizeof(float));
             // (1) temporaries of plane L on the halo-4 box, 960 positions
@@ -1847,7 +1922,9 @@ __global__ void __launch_bounds__(NT, 1) k_t1_fused_adjoint(const __grid_constan
                 phase ^= 1u;
             }
         }
+    if (stop) break;
     }  // segments
+    if (stop && tid == 0) drain_loads(bars, T1A_NSTAGE, g_wait, g_issued);
 }
 
 // Type1 imaging (kernel_type1_gpu_grad.cu:4-21) on the snapshot store:
@@ -1911,6 +1988,41 @@ struct MapKey {
 std::mutex g_map_mu;
 std::map<MapKey, CUtensorMap> g_maps;
 
+// Map of a volume of float4 cells (the interleaved model), as a 4D tensor
+// (4, ldimx, ldimy, ldimz) with box (4, bx, by, 1): a tile lands in shared
+// memory as float4 [by][bx].
+bool make_map4(CUtensorMap* m, const float4* base, const Layout& L, int bx, int by)
+{
+    auto fn = encode_fn();
+    if (!fn || !base) return false;
+    cuuint64_t dims[4] = {4, (cuuint64_t)L.ldimx, (cuuint64_t)L.ldimy, (cuuint64_t)L.ldimz};
+    cuuint64_t strides[3] = {(cuuint64_t)sizeof(float4), (cuuint64_t)L.ldimx * sizeof(float4),
+                             (cuuint64_t)L.ldimx * L.ldimy * sizeof(float4)};
+    cuuint32_t box[4] = {4, (cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float4*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+bool get_map4(CUtensorMap* out, const float4* p, const Layout& L, int bx, int by)
+{
+    MapKey k{reinterpret_cast<const float*>(p), -bx, by, L.ldimx, L.ldimy, L.ldimz};  // negative width: float4 cells
+    std::lock_guard<std::mutex> lk(g_map_mu);
+    auto it = g_maps.find(k);
+    if (it != g_maps.end()) {
+        *out = it->second;
+        return true;
+    }
+    CUtensorMap m;
+    if (!make_map4(&m, p, L, bx, by)) return false;
+    if (g_maps.size() > 4096) g_maps.clear();
+    g_maps[k] = m;
+    *out = m;
+    return true;
+}
+
 bool get_map(CUtensorMap* out, const float* p, const Layout& L, int bx, int by)
 {
     MapKey k{p, bx, by, L.ldimx, L.ldimy, L.ldimz};
@@ -1960,12 +2072,13 @@ bool prepare_device()
 {
     bool ok = err_word() != nullptr;
     ok = ok && set_smem(k_fused_forward<false>, FWD_SMEM) && set_smem(k_fused_forward<true>, FWD_SMEM);
-    ok = ok && set_smem(k_fused_adjoint<false>, ADJ_SMEM) && set_smem(k_fused_adjoint<true>, ADJ_SMEM);
-    ok = ok && set_smem(k_fused_image<false, float>, img_smem(4)) && set_smem(k_fused_image<true, float>, img_smem(4));
-    ok = ok && set_smem(k_fused_image<false, __half>, img_smem(2)) &&
-         set_smem(k_fused_image<true, __half>, img_smem(2));
-    ok = ok && set_smem(k_fused_image<false, __nv_bfloat16>, img_smem(2)) &&
-         set_smem(k_fused_image<true, __nv_bfloat16>, img_smem(2));
+    ok = ok && set_smem(k_fused_adjoint<false>, adj_smem(false)) && set_smem(k_fused_adjoint<true>, adj_smem(true));
+    ok = ok && set_smem(k_fused_image<false, float>, img_smem(4, false)) &&
+         set_smem(k_fused_image<true, float>, img_smem(4, true));
+    ok = ok && set_smem(k_fused_image<false, __half>, img_smem(2, false)) &&
+         set_smem(k_fused_image<true, __half>, img_smem(2, true));
+    ok = ok && set_smem(k_fused_image<false, __nv_bfloat16>, img_smem(2, false)) &&
+         set_smem(k_fused_image<true, __nv_bfloat16>, img_smem(2, true));
     ok = ok && set_smem(k_t1_fused_forward_x2<false>, T1F_SMEM) && set_smem(k_t1_fused_forward_x2<true>, T1F_SMEM);
     ok = ok && set_smem(k_t1_fused_adjoint<false>, T1A_SMEM) && set_smem(k_t1_fused_adjoint<true>, T1A_SMEM);
     if (!ok) cudaGetLastError();
@@ -2151,6 +2264,8 @@ Split pick_split(const Layout& L, int kind)
 
 } // namespace
 
+inline float2 pair(float c) { return make_float2(c, c); }
+
 int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
 {
     if (!layout_supported(L)) return TTI_EINVAL;
@@ -2180,6 +2295,9 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     if (s.snap && s.snap_prec != SNAP_F32 && (!s.snap_scale || !s.snap_amax)) return TTI_EINVAL;
     a.src_index = s.src_index;
     a.src_term = s.src_term;
+    a.ma = s.m.ma;
+    a.mb = s.m.mb;
+    if (!a.ma || (!s.vti && !a.mb)) return TTI_EINVAL;
     a.L = L;
     const Split sp = s.bz > 0 ? Split{s.bz, s.ztop} : choose_split(L, KIND_FWD);
     if (!split_valid(L, sp)) return TTI_EINVAL;
@@ -2193,6 +2311,18 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.invdxdy = 1.0 / (4 * s.dx * s.dy);
     a.invdydz = 1.0 / (4 * s.dy * s.dz);
     a.invdzdx = 1.0 / (4 * s.dx * s.dz);
+    const float invd[3] = {a.invdx, a.invdy, a.invdz};
+    for (int d = 0; d < 3; ++d) {
+        for (int i = 1; i <= 4; ++i) a.kd[d][i - 1] = pair(invd[d] * c1(i));
+        for (int k = 0; k < 8; ++k) a.ktap[d][k] = pair(tap(k) * invd[d]);
+    }
+    for (int j = 0; j < 8; ++j) a.kzm[j] = pair((j <= 3) ? a.invdz * c1(4 - j) : -a.invdz * c1(j - 3));
+    for (int m = -4; m <= 4; ++m) {
+        const float c = m == 0 ? 0.0f : c2(m < 0 ? -m : m);
+        a.kzx[m + 4] = pair(c * a.invdzdx);
+        a.kyz[m + 4] = pair(c * a.invdydz);
+        a.kxy[m + 4] = pair(c * a.invdxdy);
+    }
     a.err = s.err ? s.err : err_word();
     a.wave_prec = s.wave_prec;
     a.wave_scale = s.wave_scale;
@@ -2210,11 +2340,13 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
 int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
 {
     if (!layout_supported(L)) return TTI_EINVAL;
+    const bool tti = !s.vti;
+    if (!s.m.ma || (tti && !s.m.mb)) return TTI_EINVAL;
     AdjMaps tm;
-    const float* arr[ADJ_NARR] = {s.pin, s.qin, s.m.m1, s.m.m2, s.m.m3, s.m.m4, s.m.irho, s.m.rx, s.m.ry};
-    for (int k = 0; k < ADJ_NARR; ++k)
-        if (!get_map(&tm.m[k], arr[k], L, PW, PH)) return TTI_ELAUNCH;
-    if (!get_map(&tm.rz, s.m.rz, L, IW, IH)) return TTI_ELAUNCH;
+    if (!get_map(&tm.p, s.pin, L, PW, PH) || !get_map(&tm.q, s.qin, L, PW, PH) ||
+        !get_map4(&tm.ma, s.m.ma, L, PW, PH))
+        return TTI_ELAUNCH;
+    if (tti ? !get_map4(&tm.mb, s.m.mb, L, PW, PH) : !get_map(&tm.mb, s.m.irho, L, PW, PH)) return TTI_ELAUNCH;
     AdjParams a{};
     a.pout = s.pout;
     a.qout = s.qout;
@@ -2233,24 +2365,28 @@ int launch_fused_adjoint(const Layout& L, const AdjStepArgs& s, cudaStream_t st)
     a.fs = s.free_surface;
     a.sponge = s.sponge_active;
     a.dt = s.dt;
-    a.invdx = 1.0 / s.dx;
-    a.invdy = 1.0 / s.dy;
-    a.invdz = 1.0 / s.dz;
-    a.invdxy = 1.0 / (4 * s.dx * s.dy);
-    a.invdyz = 1.0 / (4 * s.dy * s.dz);
-    a.invdzx = 1.0 / (4 * s.dx * s.dz);
+    const float invd[3] = {(float)(1.0 / s.dx), (float)(1.0 / s.dy), (float)(1.0 / s.dz)};
+    const float invdxy = 1.0 / (4 * s.dx * s.dy), invdyz = 1.0 / (4 * s.dy * s.dz), invdzx = 1.0 / (4 * s.dx * s.dz);
+    for (int d = 0; d < 3; ++d)
+        for (int i = 1; i <= 4; ++i) a.kd[d][i - 1] = pair(invd[d] * c1(i));
+    for (int j = 0; j < 8; ++j) a.kzm[j] = pair((j <= 3) ? invd[2] * c1(4 - j) : -invd[2] * c1(j - 3));
+    for (int i = -4; i <= 4; ++i) {
+        const float c = i == 0 ? 0.0f : c2(i < 0 ? -i : i) * (i < 0 ? -1.0f : 1.0f);
+        a.kyz[i + 4] = pair(invdyz * c);
+        a.kzx[i + 4] = pair(invdzx * c);
+    }
+    for (int k = 1; k <= 4; ++k) a.kxy[k - 1] = pair(invdxy * c2(k));
     a.err = s.err ? s.err : err_word();
     a.wave_prec = s.wave_prec;
     a.wave_scale = s.wave_scale;
     if (a.wave_prec && !a.wave_scale) return TTI_EINVAL;
     if (!a.err) return TTI_ENOMEM;
-    const bool tti = !s.vti;
     dim3 grid(cta_count(L, sp));
     if (!kernels_prepared()) return TTI_ELAUNCH;
     if (!tti)
-        k_fused_adjoint<false><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
+        k_fused_adjoint<false><<<grid, dim3(TX, TY), adj_smem(false), st>>>(tm, a);
     else
-        k_fused_adjoint<true><<<grid, dim3(TX, TY), ADJ_SMEM, st>>>(tm, a);
+        k_fused_adjoint<true><<<grid, dim3(TX, TY), adj_smem(true), st>>>(tm, a);
     return launch_status();
 }
 
@@ -2277,7 +2413,7 @@ bool make_store_map(CUtensorMap* m, const void* base, int prec, int nx, int ny, 
 template <bool TTI, typename T>
 int launch_image_t(const ImgMaps& tm, const ImgParams& a, dim3 grid, cudaStream_t st)
 {
-    const size_t smem = img_smem(sizeof(T));
+    const size_t smem = img_smem(sizeof(T), TTI);
     k_fused_image<TTI, T><<<grid, dim3(TX, TY), smem, st>>>(tm, a);
     return launch_status();
 }
@@ -2306,14 +2442,15 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
         }
         tm.snap = it->second;
     }
-    const float* arr[IMG_NADJ] = {s.adj1, s.adj2, s.m.m1, s.m.m2, s.m.m3, s.m.m4, s.m.irho, s.m.rx, s.m.ry};
-    for (int k = 0; k < IMG_NADJ; ++k)
-        if (!get_map(&tm.a[k], arr[k], L, IW, IH)) return TTI_ELAUNCH;
+    const bool tti = !s.vti;
+    if (!s.m.ma || (tti && !s.m.mb)) return TTI_EINVAL;
+    if (!get_map(&tm.p, s.adj1, L, IW, IH) || !get_map(&tm.q, s.adj2, L, IW, IH) ||
+        !get_map4(&tm.ma, s.m.ma, L, IW, IH))
+        return TTI_ELAUNCH;
+    if (tti ? !get_map4(&tm.mb, s.m.mb, L, IW, IH) : !get_map(&tm.mb, s.m.irho, L, IW, IH)) return TTI_ELAUNCH;
     ImgParams a{};
     a.f3 = s.adj3;
     a.f4 = s.adj4;
-    a.rz = s.m.rz;
-    a.irho = s.m.irho;
     const int64_t nin = (int64_t)L.nx() * L.ny() * L.nz();
     const size_t elt = snap_elt_bytes(s.snap_prec);
     a.snap3 = static_cast<const unsigned char*>(s.store) + (size_t)s.slot * 4 * nin * elt;
@@ -2331,10 +2468,16 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
     a.hx = 1.0 / s.dx;
     a.hy = 1.0 / s.dy;
     a.hz = 1.0 / s.dz;
+    for (int r = 0; r < 4; ++r) {
+        a.kcx[r] = pair(cs(r) * a.hx);
+        a.kcy[r] = pair(cs(r) * a.hy);
+        a.kcz[r] = pair(cs(r) * a.hz);
+        a.kcxn[r] = pair(-cs(r) * a.hx);
+        a.kcyn[r] = pair(-cs(r) * a.hy);
+    }
     a.err = s.err ? s.err : err_word();
     if (!a.err) return TTI_ENOMEM;
     dim3 grid(cta_count(L, sp));
-    const bool tti = !s.vti;
     if (!kernels_prepared()) return TTI_ELAUNCH;
     switch (s.snap_prec) {
     case SNAP_F32: return tti ? launch_image_t<true, float>(tm, a, grid, st) : launch_image_t<false, float>(tm, a, grid, st);

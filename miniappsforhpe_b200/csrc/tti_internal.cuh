@@ -51,9 +51,13 @@ int launch_rho_gradient_with_base(float* grad, const float* fd1x, const float* f
                                   int ixend, int iybeg, int iyend, int izbeg, int izend, int ldimx, int ldimy,
                                   int gldx, int gldy, double dx, double dy, double dz, cudaStream_t st);
 
-// Model volumes in the reference layout, all halo'd.
+// Model volumes in the reference layout, all halo'd; the fused adjoint also
+// reads them interleaved per cell: ma = (m1, m2, m3, m4), mb = (irho, rx,
+// ry, rz), in the same layout with float4 cells.
 struct Model {
     const float *irho, *m1, *m2, *m3, *m4, *rx, *ry, *rz;
+    const float4* ma = nullptr;
+    const float4* mb = nullptr;
 };
 
 // Fused forward step (tti_fused.cu).  Reads p,q at time n from pin/qin

@@ -108,7 +108,9 @@ def test_footprint_accounts_for_snapshots_and_checkpoints():
     no_snap = P.Config(**cfg, save_snapshots=False).footprint_bytes()
     assert no_snap < ck
     # the reference kernel sequence needs its derivative volumes and scratch
-    assert P.Config(**cfg, save_snapshots=False, fused=False).footprint_bytes() - no_snap == 14 * vol
+    # (14 volumes); the fused path keeps the model a second time, interleaved
+    # in float4 cells (8 volumes)
+    assert P.Config(**cfg, save_snapshots=False, fused=False).footprint_bytes() - no_snap == 14 * vol - 8 * vol
 
 
 def test_scheme_is_validated_and_type1_needs_no_derivative_volumes():
@@ -117,10 +119,12 @@ def test_scheme_is_validated_and_type1_needs_no_derivative_volumes():
         with pytest.raises(P.TTIError) as e:
             P.Config(**base, scheme=bad).footprint_bytes()
         assert e.value.status == P.EINVAL
+    vol = 96 * 72 * 72 * 4
     fused = P.Config(**base).footprint_bytes()
-    # the centred operator's kernel sequence works on p, q, pdot, qdot alone
-    assert P.Config(**base, scheme=1, fused=False).footprint_bytes() == fused
-    assert P.Config(**base, scheme=1).footprint_bytes() == fused
+    # the centred operator's kernel sequence works on p, q, pdot, qdot alone,
+    # and neither of its paths keeps the staggered adjoint's interleaved model
+    assert P.Config(**base, scheme=1, fused=False).footprint_bytes() == fused - 8 * vol
+    assert P.Config(**base, scheme=1).footprint_bytes() == fused - 8 * vol
 
 
 def test_type1_snapshot_slots_hold_two_fields():
