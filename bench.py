@@ -12,8 +12,9 @@ CUDA events on the simulator's stream, max over ranks).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs one shot stream per GPU (independent shots, images stacked with
-one NCCL all-reduce per shot); launch it under torch.distributed.run.
+N > 1 runs one shot stream per GPU (independent shots; the image stack is
+summed over the GPUs with one NCCL all-reduce at the end of the stream);
+launch it under torch.distributed.run.
 """
 from __future__ import annotations
 
@@ -293,13 +294,17 @@ def run_ours(args):
         sim.adjoint_observed(observed)
         l2 = sim.launch_count()
         sim.image(gvp, grho)
-        if dist is not None:
-            dist.all_reduce(gvp)
         stack.add_(gvp)
         return l1 + l2
 
+    def reduce_stack():
+        # the stream's one collective: the image stack summed over the ranks
+        if dist is not None:
+            dist.all_reduce(stack)
+
     for _ in range(args.warmup):
         shot()
+    reduce_stack()
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -314,6 +319,7 @@ def run_ours(args):
     launches = 0
     for _ in range(args.steps):
         launches += shot()
+    reduce_stack()
     ev1.record(stream)
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)

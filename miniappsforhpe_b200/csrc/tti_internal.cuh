@@ -51,6 +51,19 @@ int launch_rho_gradient_with_base(float* grad, const float* fd1x, const float* f
                                   int ixend, int iybeg, int iyend, int izbeg, int izend, int ldimx, int ldimy,
                                   int gldx, int gldy, double dx, double dy, double dz, cudaStream_t st);
 
+// Receiver cells for the step kernels: the receivers lie on nz planes with
+// halo'd z index z[k]; plane k's table of receiver numbers per interior cell
+// (-1: none) starts at off[k] in xy.  Passed by value, so the plane check of
+// an output plane is a block-uniform comparison with kernel parameters.
+constexpr int kRecPlanesFolded = 8;
+struct RecMap {
+    const int* xy = nullptr;
+    int nz = 0;
+    int zlo = 1, zhi = 0;  // range of the z[k] (empty when nz = 0)
+    int z[kRecPlanesFolded] = {};
+    int off[kRecPlanesFolded] = {};
+};
+
 // Model volumes in the reference layout, all halo'd; the fused adjoint also
 // reads them interleaved per cell: ma = (m1, m2, m3, m4), mb = (irho, rx,
 // ry, rz), in the same layout with float4 cells.
@@ -88,6 +101,10 @@ struct FwdStepArgs {
     int ztop = 0;        // > 0: column tops of ztop planes, bz planes per CTA of the bottoms
     int wave_prec = 0;                 // p/q leave the step rounded to FP16 (1) or BF16 (2)
     const float* wave_scale = nullptr; // 2 power-of-two scales (p, q) of the output
+    // receivers sampled inside the step: trace[r] = -(2p + q)/3 of the
+    // incoming p, q at receiver r's cell (nullptr: not sampled here)
+    float* trace = nullptr;
+    RecMap rec{};
 };
 int launch_fused_forward(const Layout& L, const FwdStepArgs& a, cudaStream_t st);
 
@@ -112,6 +129,14 @@ struct AdjStepArgs {
     int ztop = 0;
     int wave_prec = 0;
     const float* wave_scale = nullptr;
+    // folded into the step: residual injection pdot += -2/3 v, qdot += -1/3 v
+    // at receiver r's cell, v = res[r] (- obs[r] if obs), before the update;
+    // and the source trace *srctr = p + q of the incoming state at src_index
+    const float* res = nullptr;
+    const float* obs = nullptr;
+    RecMap rec{};
+    float* srctr = nullptr;
+    int64_t src_index = -1;
 };
 int launch_fused_adjoint(const Layout& L, const AdjStepArgs& a, cudaStream_t st);
 

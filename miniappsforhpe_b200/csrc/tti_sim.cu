@@ -243,6 +243,11 @@ struct tti_sim {
     float* traces = nullptr;  // nt*nrec device
     float* resid = nullptr;   // nt*nrec device
     float* srctr = nullptr;   // nt device: adjoint p+q at the source
+    // receiver cells as per-plane tables for the fused staggered step kernels,
+    // which then sample the receivers and inject the residual themselves
+    int* rec_xy = nullptr;  // receiver number per cell of the receiver planes, -1 elsewhere
+    RecMap recmap{};        // the planes and their table offsets (kernel parameters)
+    bool rec_fold = false;
     bool model_set = false, forward_done = false;
     bool sponge_active = false;
     bool vti = false;
@@ -680,7 +685,7 @@ int wave_scale_step(tti_sim* s, WaveState& w, cudaStream_t st)
     return launch_status();
 }
 
-int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t st)
+int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t st, bool record = true)
 {
     const tti_sim_config& c = s->cfg;
     int rc0 = TTI_OK;
@@ -713,6 +718,10 @@ int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t s
     a.dy = c.dy;
     a.dz = c.dz;
     a.err = s->err;
+    if (s->rec_fold && record && s->nrec) {  // receivers sampled inside the step
+        a.trace = s->traces + (size_t)n * s->nrec;
+        a.rec = s->recmap;
+    }
     if ((rc0 = wave_scale_step(s, w, st))) return rc0;
     a.wave_prec = c.wave_precision;
     a.wave_scale = w.wscale;
@@ -726,7 +735,8 @@ int fused_forward_step(tti_sim* s, WaveState& w, int n, int slot, cudaStream_t s
     return TTI_OK;
 }
 
-int fused_adjoint_step(tti_sim* s, cudaStream_t st)
+int fused_adjoint_step(tti_sim* s, cudaStream_t st, const float* res = nullptr, const float* obs = nullptr,
+                       float* srctr = nullptr)
 {
     const tti_sim_config& c = s->cfg;
     WaveState& w = s->w;
@@ -749,6 +759,11 @@ int fused_adjoint_step(tti_sim* s, cudaStream_t st)
     a.dy = c.dy;
     a.dz = c.dz;
     a.err = s->err;
+    a.res = res;
+    a.obs = obs;
+    if (res) a.rec = s->recmap;
+    a.srctr = srctr;
+    a.src_index = srctr ? s->src_index : -1;
     int rc = wave_scale_step(s, w, st);
     if (rc) return rc;
     a.wave_prec = c.wave_precision;
@@ -810,7 +825,7 @@ int image_step(tti_sim* s, int slot, cudaStream_t st)
 
 int receivers_step(tti_sim* s, WaveState& w, int n, cudaStream_t st)
 {
-    if (!s->nrec) return TTI_OK;
+    if (!s->nrec || s->rec_fold) return TTI_OK;  // folded: the fused step samples them
     k_receivers<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->traces + (size_t)n * s->nrec, w.p, w.q, s->rec, s->nrec);
     s->launches++;
     return launch_status();
@@ -858,20 +873,24 @@ int adjoint_unit(tti_sim* s, int n, int seg_start, bool observed, cudaStream_t s
 {
     const tti_sim_config& c = s->cfg;
     int r = TTI_OK;
-    if (s->src_index >= 0) {
-        k_source_trace<<<1, 1, 0, st>>>(s->srctr + n, s->w.p, s->w.q, s->src_index);
-        s->launches++;
-    }
-    if (s->nrec) {
-        const float* obs = observed ? s->resid + (size_t)n * s->nrec : nullptr;
-        const float* res = observed ? s->traces + (size_t)n * s->nrec : s->resid + (size_t)n * s->nrec;
-        k_inject_residual<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->w.pd, s->w.qd, s->rec, res, obs, s->nrec);
-        s->launches++;
-    }
-    if (!c.fused) {
-        if ((r = adjoint_per_kernel_step(s, st))) return r;
+    const float* obs = (s->nrec && observed) ? s->resid + (size_t)n * s->nrec : nullptr;
+    const float* res = !s->nrec ? nullptr : observed ? s->traces + (size_t)n * s->nrec : s->resid + (size_t)n * s->nrec;
+    if (s->rec_fold) {  // source trace and residual injection inside the fused step
+        if ((r = fused_adjoint_step(s, st, res, obs, s->src_index >= 0 ? s->srctr + n : nullptr))) return r;
     } else {
-        if ((r = fused_adjoint_step(s, st))) return r;
+        if (s->src_index >= 0) {
+            k_source_trace<<<1, 1, 0, st>>>(s->srctr + n, s->w.p, s->w.q, s->src_index);
+            s->launches++;
+        }
+        if (s->nrec) {
+            k_inject_residual<<<(s->nrec + 255) / 256, 256, 0, st>>>(s->w.pd, s->w.qd, s->rec, res, obs, s->nrec);
+            s->launches++;
+        }
+        if (!c.fused) {
+            if ((r = adjoint_per_kernel_step(s, st))) return r;
+        } else {
+            if ((r = fused_adjoint_step(s, st))) return r;
+        }
     }
     if (with_image && n % c.xcorr_step == 0 && (r = image_step(s, (n - seg_start) / c.xcorr_step, st))) return r;
     return launch_status();
@@ -1122,9 +1141,52 @@ int tti_sim_set_receivers(tti_sim* s, int nrec, const int* ixyz)
             *p = nullptr;
         }
     }
+    for (void** p : {(void**)&s->rec_xy}) {
+        if (*p) {
+            cudaFreeAsync(*p, s->stream);
+            for (auto& a : s->allocs)
+                if (a == *p) a = nullptr;
+            *p = nullptr;
+        }
+    }
+    s->rec_fold = false;
+    s->recmap = RecMap{};
     s->nrec = nrec;
     if (nrec == 0) return TTI_OK;
     int rc = s->alloc((void**)&s->rec, nrec * sizeof(int64_t));
+    // The fused staggered step kernels sample the receivers and inject the
+    // residual themselves when the receivers lie on a few planes (a table of
+    // nx*ny receiver numbers per plane); otherwise separate kernels do it.
+    const tti_sim_config& c = s->cfg;
+    std::vector<int> plane_of(c.nz, -1);
+    int nplanes = 0;
+    for (int r = 0; r < nrec; ++r) {
+        int& pl = plane_of[ixyz[3 * r + 2]];
+        if (pl < 0) pl = nplanes++;
+    }
+    if (!rc && c.fused && c.scheme == 0 && nplanes <= kRecPlanesFolded) {
+        const size_t plane = (size_t)c.nx * c.ny;
+        std::vector<int> xy(nplanes * plane, -1);
+        RecMap m{};
+        m.nz = nplanes;
+        m.zlo = 1 << 30;
+        m.zhi = -1;
+        for (int iz = 0; iz < c.nz; ++iz)
+            if (plane_of[iz] >= 0) {
+                m.z[plane_of[iz]] = iz + kRadius;
+                m.off[plane_of[iz]] = (int)(plane_of[iz] * plane);
+                m.zlo = std::min(m.zlo, iz + kRadius);
+                m.zhi = std::max(m.zhi, iz + kRadius);
+            }
+        for (int r = 0; r < nrec; ++r)
+            xy[plane_of[ixyz[3 * r + 2]] * plane + (size_t)ixyz[3 * r + 1] * c.nx + ixyz[3 * r]] = r;
+        rc = s->alloc((void**)&s->rec_xy, xy.size() * sizeof(int));
+        if (!rc && cudaMemcpy(s->rec_xy, xy.data(), xy.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = cuda_rc(cudaGetLastError());
+        m.xy = s->rec_xy;
+        s->recmap = m;
+        s->rec_fold = !rc;
+    }
     if (!rc) rc = s->alloc((void**)&s->traces, (size_t)nrec * s->cfg.nt * sizeof(float));
     if (!rc) rc = s->alloc((void**)&s->resid, (size_t)nrec * s->cfg.nt * sizeof(float));
     if (!rc && cudaMemcpy(s->rec, idx.data(), nrec * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -1246,7 +1308,7 @@ static int sim_adjoint(tti_sim* s, const float* residual, int residual_on_device
                     if ((r = restore_checkpoint(s, s->rw, k, st))) return r;
                     for (int n = a; n < b; ++n) {
                         const int slot = (n % c.xcorr_step == 0) ? (n - a) / c.xcorr_step : -1;
-                        if ((r = fused_forward_step(s, s->rw, n, slot, st))) return r;
+                        if ((r = fused_forward_step(s, s->rw, n, slot, st, false))) return r;
                     }
                 }
                 return adjoint_steps(b - 1, a, a, st);
@@ -1534,7 +1596,7 @@ int shot_advance(tti_sim* s, cudaStream_t st, int64_t max_units, int64_t* done)
                 const int n = s->sh_n;
                 if (n == a && (rc = restore_checkpoint(s, s->rw, s->sh_seg, st))) return rc;
                 const int slot = (n % c.xcorr_step == 0) ? (n - a) / c.xcorr_step : -1;
-                if ((rc = fused_forward_step(s, s->rw, n, slot, st))) return rc;
+                if ((rc = fused_forward_step(s, s->rw, n, slot, st, false))) return rc;
                 ++*done;
                 if (++s->sh_n == b) {
                     s->sh_recomp = false;
