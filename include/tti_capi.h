@@ -535,6 +535,71 @@ double tti_server_now(tti_server* srv);
 /* Runs every submitted shot to completion, then releases the server. */
 int tti_server_destroy(tti_server* srv);
 
+/* ------------------------------------------------------------------------
+ * 5. Elastic step kernels of the reference's simulator3 (its eTTI proxy),
+ * with the reference's stand-in constants (first-derivative and
+ * interpolation tables {1.01, 2.01, 3.01, 4.01}, inverse spacings 1.01 and
+ * 2.01 or 2.02 in x and y, zprime[iz] in z) and arithmetic.  Volumes are
+ * FP32, x fastest, radius-4 halo on every axis, interior [4, 4+n-1] per
+ * axis, idx = (iz*ldimy + iy)*ldimx + ix, ldimx >= nx + 8, ldimy >= ny + 8,
+ * and the z allocation holds nz + 8 planes; zprime is indexed by the halo'd
+ * z.  The reference launches need nx a multiple of 32 and ny of 16 (its
+ * blocks check no bounds); these take any size and write interior cells
+ * only.  stream 0 is the default stream. */
+
+/* Replaces vgPlainLoop (simulator3/simulator3SetUp.cu:1364-1386): the six
+ * strain volumes d4..d9 from the velocities f1, f2, f3. */
+int tti_e3_launch_vgplain(const float* f1, const float* f2, const float* f3, float* d4, float* d5, float* d6,
+                          float* d7, float* d8, float* d9, const float* zprime, int nx, int ny, int nz, int ldimx,
+                          int ldimy, tti_stream_t stream);
+
+/* Replaces sPlainLoop (simulator3/simulator3SetUp.cu:1127-1216): the six
+ * z-mixed precomputes into f10_21[0..11] (the reference's f10 .. f21, in its
+ * 64-plane z blocks, whose first planes it weighs differently), then the
+ * stress update f4..f9 += C:strain with M[0..20] = M1..M21 and the strains
+ * f1_1, f1_2, f1_3, f2_2, f2_3, f3_3 (the simulator passes d4 .. d9). */
+int tti_e3_launch_splain(float* f4, float* f5, float* f6, float* f7, float* f8, float* f9, const float* const* M,
+                         const float* f1_1, const float* f1_2, const float* f1_3, const float* f2_2,
+                         const float* f2_3, const float* f3_3, float* const* f10_21, int nx, int ny, int nz,
+                         int ldimx, int ldimy, tti_stream_t stream);
+
+/* Replaces vPlainLoop (simulator3/simulator3SetUp.cu:1105-1125): the
+ * velocity update f1..f3 += 2*M22 * div(stress f4..f9). */
+int tti_e3_launch_vplain(float* f1, float* f2, float* f3, const float* f4, const float* f5, const float* f6,
+                         const float* f7, const float* f8, const float* f9, const float* M22, const float* zprime,
+                         int nx, int ny, int nz, int ldimx, int ldimy, tti_stream_t stream);
+
+/* Replaces mirror_s / mirror_v (simulator3/simulator3SetUp.cu:1425-1492):
+ * on nfields (1..6) volumes, plane izbeg set to zero and planes 0..izbeg-1
+ * to the negated mirror 2*izbeg - iz, whole planes (halos included);
+ * ldimz (the planes allocated) bounds the mirror: 2*izbeg < ldimz. */
+int tti_e3_launch_mirror(float* const* fields, int nfields, int ldimx, int ldimy, int ldimz, int izbeg,
+                         tti_stream_t stream);
+
+/* Replaces update_gv / update_g_v (simulator3/simulator3SetUp.cu:1494-1538):
+ * the velocity image g1 += a_v1 * snap_v1 + a_v3 * snap_v3 over the nx*ny*nz
+ * interior, g1 and the snapshots halo-free with leading dimensions g_ldimx,
+ * g_ldimy, the adjoint velocities halo'd (ldimx, ldimy).  The density image
+ * of the same schedule (update_g_r_impl, :2091-2128) is the TTI density
+ * gradient with the elastic volumes in its argument slots:
+ * tti_launch_update_rho_gradient_rho. */
+int tti_e3_launch_update_gv(float* g1, const float* snap_v1, const float* snap_v3, const float* a_v1,
+                            const float* a_v3, int nx, int ny, int nz, int ldimx, int ldimy, int g_ldimx, int g_ldimy,
+                            tti_stream_t stream);
+
+/* Replaces compute_p_kernel (simulator3/simulator3SetUp.cu:275-289) over n
+ * cells: p = -(2 f4 + 3 f5 + 4 f6 + 5 f7 + 6 f8 + 7 f9) / 27. */
+int tti_e3_launch_compute_p(float* p, const float* f4, const float* f5, const float* f6, const float* f7,
+                            const float* f8, const float* f9, int64_t n, tti_stream_t stream);
+
+/* Replaces init_cijs_kernel (simulator3/simulator3SetUp.cu:229-273): the
+ * stand-in model M[0..21] = M1..M22, the strains d4_9[0..5] = d4..d9 and
+ * zprime, from cos/sin of the halo'd cell indices, over the interior x range
+ * and every y and z of the allocation (ldimz planes), as the reference's
+ * launch covers them. */
+int tti_e3_launch_init_model(float* const* M22, float* const* d4_9, float* zprime, int nx, int ldimx, int ldimy,
+                             int ldimz, tti_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

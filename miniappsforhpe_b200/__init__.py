@@ -119,6 +119,13 @@ _SIGS = {
     "tti_snap_start_read": [V, V, V],
     "tti_snap_finish_read": [V, V],
     "tti_snap_count": [V],
+    "tti_e3_launch_vgplain": [V] * 10 + [I] * 5 + [V],
+    "tti_e3_launch_splain": [V] * 14 + [I] * 5 + [V],
+    "tti_e3_launch_vplain": [V] * 11 + [I] * 5 + [V],
+    "tti_e3_launch_mirror": [V, I, I, I, I, I, V],
+    "tti_e3_launch_update_gv": [V] * 5 + [I] * 7 + [V],
+    "tti_e3_launch_compute_p": [V] * 7 + [L64, V],
+    "tti_e3_launch_init_model": [V] * 3 + [I] * 4 + [V],
 }
 
 

@@ -17,7 +17,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtti_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
-SOURCES = ["tti_kernels.cu", "tti_fused.cu", "tti_sim.cu", "tti_snap.cu", "tti_noalloc.cu", "tti_serve.cu", "tti_type1.cu"]
+SOURCES = ["tti_kernels.cu", "tti_fused.cu", "tti_sim.cu", "tti_snap.cu", "tti_noalloc.cu", "tti_serve.cu", "tti_type1.cu",
+           "tti_elastic.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "--diag-suppress=177", f"-I{os.path.join(ROOT, 'include')}"]

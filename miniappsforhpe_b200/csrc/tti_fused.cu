@@ -262,16 +262,7 @@ struct FwdParams {
     int* err;
     int wave_prec;            // 0, or p/q rounded to FP16 (1) / BF16 (2) each step
     const float* wave_scale;  // 2 scales (p, q) of this step's output
-    // stencil coefficients with the grid spacings folded in, as (c, c) pairs
-    float2 kd[3][4];    // c1(i)/dx, /dy, /dz, i = 1..4 (staggered D-)
-    float2 ktap[3][8];  // tap(k)/dx, /dy, /dz, k = 0..7 (staggered D+ over consecutive points)
-    float2 kzm[8];      // D- z scatter into queue slot j: +c1(4-j)/dz (j <= 3), -c1(j-3)/dz
-    float2 kzx[9];      // c2(|m|)/(4 dz dx) for plane offset m = -4..4
-    float2 kyz[9];      // c2(|m|)/(4 dy dz)
-    float2 kxy[9];      // c2(|k|)/(4 dx dy) for diagonal offset k = -4..4
-    const float4* ma;   // (m1, m2, m3, m4) per cell
-    const float4* mb;   // (irho, rx, ry, rz) per cell (TTI)
-    float* trace;       // receivers of this step (nullptr: not sampled here)
+    float* trace;             // receivers of this step (nullptr: not sampled here)
     RecMap rec;
 };
 
@@ -2335,9 +2326,6 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     if (s.snap && s.snap_prec != SNAP_F32 && (!s.snap_scale || !s.snap_amax)) return TTI_EINVAL;
     a.src_index = s.src_index;
     a.src_term = s.src_term;
-    a.ma = s.m.ma;
-    a.mb = s.m.mb;
-    if (!a.ma || (!s.vti && !a.mb)) return TTI_EINVAL;
     a.trace = s.trace;
     a.rec = s.rec;
     if (a.trace && !a.rec.xy) return TTI_EINVAL;
@@ -2354,18 +2342,6 @@ int launch_fused_forward(const Layout& L, const FwdStepArgs& s, cudaStream_t st)
     a.invdxdy = 1.0 / (4 * s.dx * s.dy);
     a.invdydz = 1.0 / (4 * s.dy * s.dz);
     a.invdzdx = 1.0 / (4 * s.dx * s.dz);
-    const float invd[3] = {a.invdx, a.invdy, a.invdz};
-    for (int d = 0; d < 3; ++d) {
-        for (int i = 1; i <= 4; ++i) a.kd[d][i - 1] = pair(invd[d] * c1(i));
-        for (int k = 0; k < 8; ++k) a.ktap[d][k] = pair(tap(k) * invd[d]);
-    }
-    for (int j = 0; j < 8; ++j) a.kzm[j] = pair((j <= 3) ? a.invdz * c1(4 - j) : -a.invdz * c1(j - 3));
-    for (int m = -4; m <= 4; ++m) {
-        const float c = m == 0 ? 0.0f : c2(m < 0 ? -m : m);
-        a.kzx[m + 4] = pair(c * a.invdzdx);
-        a.kyz[m + 4] = pair(c * a.invdydz);
-        a.kxy[m + 4] = pair(c * a.invdxdy);
-    }
     a.err = s.err ? s.err : err_word();
     a.wave_prec = s.wave_prec;
     a.wave_scale = s.wave_scale;

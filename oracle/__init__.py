@@ -410,3 +410,135 @@ def rtm_shot_t1(o, lay, m, ab, cfg, src, wavelet, rec, residual=None):
             o.t1_grad(lay, snaps[n][0], snaps[n][1], gvp, a3, a4)
     o.finalize_vp_gradient(lay, m["m3"], gvp, np.float32(cfg.dt * cfg.xcorr_step))
     return {"traces": traces, "f3": f3, "grad_vp": gvp.reshape(lay.nz, lay.ny, lay.nx)}
+
+
+# --- simulator3 (the elastic eTTI proxy) --------------------------------------
+_E3_SIGS = {
+    "orc_e3_vgplain": [V] * 10 + [I] * 5,
+    "orc_e3_precompute": [V] * 3 + [I] * 8,
+    "orc_e3_splain": [V] * 14 + [I] * 5,
+    "orc_e3_vplain": [V] * 11 + [I] * 5,
+    "orc_e3_mirror": [V, I, I, I, I],
+    "orc_e3_update_gv": [V] * 5 + [I] * 7,
+    "orc_e3_pressure": [V] * 7 + [L],
+    "orc_e3_init_model": [V] * 3 + [I] * 4,
+}
+
+
+def _parr(vols):
+    return (V * len(vols))(*[_p(v) for v in vols])
+
+
+class ElasticOracle:
+    """FP32 restatement of the simulator3 step kernels (``elastic_oracle.c``).
+
+    Volumes are numpy arrays of ``Layout.shape``; ``M`` lists M1..M21 (or
+    M1..M22), ``pre`` the twelve z-mixed volumes f10..f21."""
+
+    def __init__(self):
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run `make -C oracle`")
+        self.lib = C.CDLL(LIB_PATH)
+        self.fn = {}
+        for name, sig in _E3_SIGS.items():
+            f = getattr(self.lib, name)
+            f.argtypes = sig
+            f.restype = None
+            self.fn[name] = f
+
+    def vgplain(self, lay, f1, f2, f3, d, zprime):
+        self.fn["orc_e3_vgplain"](_p(f1), _p(f2), _p(f3), *[_p(x) for x in d], _p(zprime), lay.nx, lay.ny, lay.nz,
+                                  lay.ldimx, lay.ldimy)
+
+    def precompute(self, lay, src, xz, yz, xs, ys, zs):
+        self.fn["orc_e3_precompute"](_p(src), _p(xz), _p(yz), xs, ys, zs, lay.nx, lay.ny, lay.nz, lay.ldimx,
+                                     lay.ldimy)
+
+    def splain(self, lay, s, M, d, pre):
+        """s = f4..f9, d = (d4..d9) as (f1_1, f1_2, f1_3, f2_2, f2_3, f3_3)."""
+        m, p = _parr(M[:21]), _parr(pre)
+        self.fn["orc_e3_splain"](*[_p(x) for x in s], C.addressof(m), *[_p(x) for x in d], C.addressof(p), lay.nx,
+                                 lay.ny, lay.nz, lay.ldimx, lay.ldimy)
+
+    def vplain(self, lay, v, s, M22, zprime):
+        self.fn["orc_e3_vplain"](*[_p(x) for x in v], *[_p(x) for x in s], _p(M22), _p(zprime), lay.nx, lay.ny,
+                                 lay.nz, lay.ldimx, lay.ldimy)
+
+    def mirror(self, lay, fields, izbeg=RADIUS):
+        f = _parr(fields)
+        self.fn["orc_e3_mirror"](C.addressof(f), len(fields), lay.ldimx, lay.ldimy, izbeg)
+
+    def update_gv(self, lay, g, s1, s3, a1, a3):
+        self.fn["orc_e3_update_gv"](_p(g), _p(s1), _p(s3), _p(a1), _p(a3), lay.nx, lay.ny, lay.nz, lay.ldimx,
+                                    lay.ldimy, lay.nx, lay.ny)
+
+    def pressure(self, p, s):
+        self.fn["orc_e3_pressure"](_p(p), *[_p(x) for x in s], p.size)
+
+    def init_model(self, lay, M, d, zprime):
+        m, dd = _parr(M), _parr(d)
+        self.fn["orc_e3_init_model"](C.addressof(m), C.addressof(dd), _p(zprime), lay.nx, lay.ldimx, lay.ldimy,
+                                     lay.ldimz)
+
+
+def e3_execute(lay, niter, xcorr_step, press=500.0, adjoint=True, d123=(1.0, 1.0, 1.0)):
+    """simulator3SetUp::execute (simulator3/simulator3SetUp.cu:2181-2657) on
+    one subdomain, with the oracle: the stand-in model, the stress source at
+    the grid centre, the forward steps (velocity update, free-surface
+    mirrors, strains, stress update, pressure) with snapshots of the
+    velocities every ``xcorr_step`` steps, then the adjoint steps in the
+    reverse order with the velocity and density images.  Returns a dict of
+    the final volumes and images."""
+    e, o = ElasticOracle(), Oracle("f32")
+    z = lay.zeros
+    M = [z() for _ in range(22)]
+    d = [z() for _ in range(6)]
+    zprime = np.zeros(lay.ldimz, np.float32)
+    e.init_model(lay, M, d, zprime)
+    v = [z() for _ in range(3)]
+    s = [z() for _ in range(6)]
+    pre = [z() for _ in range(12)]
+    p = z()
+    c = tuple(n // 2 + RADIUS for n in (lay.nx, lay.ny, lay.nz))
+    for k in range(6):  # init_src_kernel (:291-300)
+        s[k][c[2], c[1], c[0]] = np.float32(press) * np.float32(k + 1)
+    I = lay.interior
+    snaps = {}
+    nxt = 0
+    for it in range(niter):
+        e.vplain(lay, v, s, M[21], zprime)
+        e.mirror(lay, s)
+        e.mirror(lay, s)
+        e.mirror(lay, v)
+        e.mirror(lay, v)
+        e.vgplain(lay, *v, d, zprime)
+        e.splain(lay, s, M, d, pre)
+        e.pressure(p, s)
+        if adjoint and it == nxt:
+            snaps[it] = (np.ascontiguousarray(v[0][I]), np.ascontiguousarray(v[2][I]))
+            nxt += xcorr_step
+    out = {"v": [x.copy() for x in v], "s": [x.copy() for x in s], "d": [x.copy() for x in d], "p": p.copy(),
+           "pre": [x.copy() for x in pre]}
+    if not adjoint:
+        return out
+    g1 = np.zeros((lay.nz, lay.ny, lay.nx), np.float32)
+    g2 = np.zeros((lay.nz, lay.ny, lay.nx), np.float32)
+    nxt -= xcorr_step
+    for it in range(niter - 1, -1, -1):
+        e.splain(lay, s, M, d, pre)
+        e.vgplain(lay, *v, d, zprime)
+        e.mirror(lay, s)
+        e.mirror(lay, s)
+        e.mirror(lay, v)
+        e.mirror(lay, v)
+        e.vplain(lay, v, s, M[21], zprime)
+        if it == nxt:
+            e.update_gv(lay, g1, snaps[it][0], snaps[it][1], v[0], v[2])
+            # update_g_r_impl (:2091-2128): the TTI density gradient with
+            # d4..d9, f4, f6, M18 (as 1/rho), M1..M4 and M5..M7 (as rx, ry, rz)
+            o.rho_gradient(lay, g2, {"d1x": d[0], "d1y": d[1], "d1z": d[2], "d2x": d[3], "d2y": d[4], "d2z": d[5]},
+                           s[0], s[2], {"irho": M[17], "m1": M[0], "m2": M[1], "m3": M[2], "m4": M[3], "rx": M[4],
+                                        "ry": M[5], "rz": M[6]}, d123, lay.nx, lay.ny)
+            nxt -= xcorr_step
+    out.update({"v_adj": v, "s_adj": s, "g1": g1, "g2": g2})
+    return out
