@@ -7,11 +7,14 @@ a z extent that crosses one of its 64-plane blocks; the mirrors, the
 pressure and the stand-in model against their formulas (:229-300,
 :1387-1492); and the composed schedule (:2181-2657) for finite images.
 """
+import os
+
 import numpy as np
 import pytest
 
 from oracle import ElasticOracle, Layout, e3_execute
 
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INT = np.array([1.01, 2.01, 3.01, 4.01], np.float32)
 
 
@@ -124,3 +127,13 @@ def test_composed_schedule_images():
     assert np.isfinite(out["g1"]).all() and np.abs(out["g1"]).max() > 0
     inner = out["g2"][:, :, 4:lay.nx - 4]
     assert np.isfinite(inner).all() and np.abs(inner).max() > 0
+
+
+def test_bench_cpu_sample_of_the_elastic_steps():
+    import sys
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    d = bench.elastic_cpu_sample(n=24, steps=1)
+    assert d["value"] > 0 and d["kind"] == "port" and d["cores"] >= 1
