@@ -457,10 +457,13 @@ def run_ours(args):
         b_step = B_VTI if vti else (B_FWD if kind == "forward" else B_ADJ)
     alg_bytes = b_step * npts
     achieved = alg_bytes / per_launch_s / 1e9 if kn else None
-    traffic = ncu_traffic().get(f"{'type1_' if t1 else ''}{kind}_dram_bytes_per_launch_{nx}x{ny}x{nz}")
+    tkey = f"{'type1_' if t1 else ''}{kind}"
+    tr = ncu_traffic()
+    traffic = tr.get(f"{tkey}_dram_bytes_per_launch_{nx}x{ny}x{nz}")
     roofline = {"kernel": f"fused {'type1 ' if t1 else ''}{kind} step", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                "traffic": traffic, "traffic_split": tr.get(f"{tkey}_split_{nx}x{ny}x{nz}"),
+                "alg_bytes_per_launch": alg_bytes,
                 "avg_launch_ms": per_launch_s * 1e3, "launches": kn}
     passes = {k: {"total_ms": v[0] / args.steps, "launches_per_shot": v[1] / args.steps}
               for k, v in times.items()}

@@ -474,10 +474,12 @@ __global__ void __launch_bounds__(NT, 1)
                 dys[r * TX + c] = in ? make_float2(acc[0] * irv, acc[1] * irv) : make_float2(0.0f, 0.0f);
             };
             dx_at(ty, tx);
-            // the (IW-TX) x TY halo columns, by whole warps
+            // the halos by whole warps, spread so that no warp does more than
+            // three tile cells: the (IW-TX) x TY halo columns by warps 0..3,
+            // the (IH-TY) halo rows by warps 4..11
             if (tid < (IW - TX) * TY) dx_at(tid / (IW - TX), TX + tid % (IW - TX));
             dy_at(ty, tx);
-            if (ty < IH - TY) dy_at(ty + TY, tx);
+            if (ty >= 4 && ty < 4 + IH - TY) dy_at(ty - 4 + TY, tx);
             __syncthreads();
             float snapv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             if (owner) {
@@ -1294,9 +1296,11 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             ys[r * TX + c] = make_float4(acc.x, acc.y, t2.x, t2.y);
         };
         xt_at(ty, tx);
+        // halos spread over warps 0..3 (x) and 4..11 (y): at most three
+        // tile cells per warp
         if (tid < (IW - TX) * TY) xt_at(tid / (IW - TX), TX + tid % (IW - TX));
         yt_at(ty, tx);
-        if (ty < IH - TY) yt_at(ty + TY, tx);
+        if (ty >= 4 && ty < 4 + IH - TY) yt_at(ty - 4 + TY, tx);
         // (2) column values: z temporaries, buoyancy, D- z stage of the stored p/q
         {
             const float4 g = geo(kc);
