@@ -17,6 +17,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <initializer_list>
+
+#include <cuda_pipeline.h>
 
 #include "tti_common.cuh"
 
@@ -89,10 +92,57 @@ __device__ __forceinline__ void zshift(float (&w)[9], const float* __restrict__ 
     w[8] = __ldg(p + next);
 }
 
+// drv1_8 on a shared-memory tile (stride s between taps).
+template <bool SHIFT>
+__device__ __forceinline__ float drv8s(const float* p, int s)
+{
+    constexpr int is = SHIFT ? -1 : 0;
+    float d = e3_df(0) * (p[(is + 1) * s] - p[is * s]);
+#pragma unroll
+    for (int i = 1; i < 4; ++i) d += e3_df(i) * (p[(is + i + 1) * s] - p[(is - i) * s]);
+    return d;
+}
+
+// Stage rows ys .. ys+R-1, columns xs .. xs+C-1 of one plane into t (zero
+// past the allocation's row or plane end; no output reads those cells).
+template <int R, int C>
+__device__ __forceinline__ void stage_tile(float (&t)[R][C], const float* __restrict__ plane, int xs, int ys,
+                                           const E3Grid& g, int tid)
+{
+    for (int e = tid; e < R * C; e += E3X * E3Y) {
+        const int r = e / C, c = e - r * C, x = xs + c, y = ys + r;
+        t[r][c] = (x < g.ldimx && y < g.ldimy) ? __ldg(plane + (int64_t)y * g.ldimx + x) : 0.0f;
+    }
+}
+
+// The same, issued as asynchronous copies (LDGSTS) of V floats (1, or 4
+// when ldimx is a multiple of 4 and the volumes are 16-byte aligned: then
+// xs being a multiple of 4, a chunk lies wholly inside or wholly past a
+// row's end) into t; the caller commits and waits.  Cells past the
+// allocation's row or plane end are zeroed directly.
+template <int V, int R, int C>
+__device__ __forceinline__ void stage_tile_async(float (&t)[R][C], const float* __restrict__ plane, int xs, int ys,
+                                                 const E3Grid& g, int tid)
+{
+    static_assert(C % V == 0, "rows of whole chunks");
+    constexpr int CC = C / V;
+    for (int e = tid; e < R * CC; e += E3X * E3Y) {
+        const int r = e / CC, c = V * (e - r * CC), x = xs + c, y = ys + r;
+        if (x < g.ldimx && y < g.ldimy) {
+            __pipeline_memcpy_async(&t[r][c], plane + (int64_t)y * g.ldimx + x, V * sizeof(float));
+        } else {
+#pragma unroll
+            for (int k = 0; k < V; ++k) t[r][c + k] = 0.0f;
+        }
+    }
+}
+
 // vgPlainKernel (simulator3SetUp.cu:1218-1362): the six strain volumes.  A
-// thread walks E3ZC planes of its column with the z taps of f1, f2, f3 in
-// register windows (one load per plane and field, as the reference's
-// queues); the x/y taps come through L1.
+// block walks E3ZC planes of a 32x8 column tile: the x/y taps of each plane
+// come from shared-memory tiles of f1, f2, f3 with a halo of 4, the z taps
+// from per-thread register windows (one load per plane and field), as the
+// reference's shared planes and queues do.
+template <int V>
 __global__ void __launch_bounds__(E3X* E3Y) k_e3_vgplain(const float* __restrict__ f1, const float* __restrict__ f2,
                                                         const float* __restrict__ f3, float* __restrict__ d4,
                                                         float* __restrict__ d5, float* __restrict__ d6,
@@ -100,15 +150,17 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vgplain(const float* __restrict
                                                         float* __restrict__ d9, const float* __restrict__ zprime,
                                                         E3Grid g)
 {
-    const int ix = 4 + blockIdx.x * E3X + threadIdx.x, iy = 4 + blockIdx.y * E3Y + threadIdx.y;
-    if (ix >= 4 + g.nx || iy >= 4 + g.ny) return;
+    __shared__ __align__(16) float t1[2][E3Y + 8][E3X + 8], t2[2][E3Y + 8][E3X + 8], t3[2][E3Y + 8][E3X + 8];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * E3X + tx;
+    const int x0 = 4 + blockIdx.x * E3X, y0 = 4 + blockIdx.y * E3Y;
+    const int ix = x0 + tx, iy = y0 + ty;
+    const bool act = ix < 4 + g.nx && iy < 4 + g.ny;
     const float invd1 = 1.01f, invd2 = 2.02f;
-    const int64_t sy = g.ldimx, sz = (int64_t)g.ldimx * g.ldimy;
+    const int64_t sz = (int64_t)g.ldimx * g.ldimy;
     const int z0 = 4 + blockIdx.z * E3ZC, z1 = min(z0 + E3ZC, 4 + g.nz);
-    float w1[9], w2[9], w3[9];  // planes iz-4 .. iz+4
-    {
+    float w1[9] = {}, w2[9] = {}, w3[9] = {};  // planes iz-4 .. iz+4
+    if (act) {
         const int64_t i0 = g.idx(ix, iy, z0 - 4);
-        w1[8] = w2[8] = w3[8] = 0.0f;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             w1[k + 1] = __ldg(f1 + i0 + k * sz);
@@ -116,32 +168,57 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vgplain(const float* __restrict
             w3[k + 1] = __ldg(f3 + i0 + k * sz);
         }
     }
-    for (int iz = z0; iz < z1; ++iz) {
+    // planes double-buffered: plane iz+1 is copied in while plane iz is used
+    auto stage = [&](int b, int iz) {
+        const int64_t pb = (int64_t)iz * sz;
+        stage_tile_async<V>(t1[b], f1 + pb, x0 - 4, y0 - 4, g, tid);
+        stage_tile_async<V>(t2[b], f2 + pb, x0 - 4, y0 - 4, g, tid);
+        stage_tile_async<V>(t3[b], f3 + pb, x0 - 4, y0 - 4, g, tid);
+        __pipeline_commit();
+    };
+    if (z0 < z1) stage(0, z0);
+    for (int iz = z0, b = 0; iz < z1; ++iz, b ^= 1) {
         const int64_t i = g.idx(ix, iy, iz);
-        zshift(w1, f1, i + 4 * sz);
-        zshift(w2, f2, i + 4 * sz);
-        zshift(w3, f3, i + 4 * sz);
-        const float d19 = drv8<false>(f1 + i, 1), d20 = drv8<false>(f2 + i, sy), d21 = zdrv(w3, false);
-        const float d22 = drv8<true>(f1 + i, sy), d23 = drv8<true>(f2 + i, 1), d24 = zdrv(w1, true);
-        const float d25 = drv8<true>(f3 + i, 1), d26 = zdrv(w2, true), d27 = drv8<true>(f3 + i, sy);
-        const float zpr = __ldg(zprime + iz);
-        d4[i] = invd1 * d19;
-        d5[i] = invd2 * d22 + invd1 * d23;
-        d6[i] = zpr * d24 + invd1 * d25;
-        d7[i] = invd2 * d20;
-        d8[i] = zpr * d26 + invd2 * d27;
-        d9[i] = zpr * d21;
+        if (iz + 1 < z1) stage(b ^ 1, iz + 1);
+        if (act) {
+            zshift(w1, f1, i + 4 * sz);
+            zshift(w2, f2, i + 4 * sz);
+            zshift(w3, f3, i + 4 * sz);
+        }
+        __pipeline_wait_prior(iz + 1 < z1 ? 1 : 0);
+        __syncthreads();
+        if (act) {
+            constexpr int S = E3X + 8;
+            const float* c1 = &t1[b][ty + 4][tx + 4];
+            const float* c2 = &t2[b][ty + 4][tx + 4];
+            const float* c3 = &t3[b][ty + 4][tx + 4];
+            const float d19 = drv8s<false>(c1, 1), d20 = drv8s<false>(c2, S), d21 = zdrv(w3, false);
+            const float d22 = drv8s<true>(c1, S), d23 = drv8s<true>(c2, 1), d24 = zdrv(w1, true);
+            const float d25 = drv8s<true>(c3, 1), d26 = zdrv(w2, true), d27 = drv8s<true>(c3, S);
+            const float zpr = __ldg(zprime + iz);
+            d4[i] = invd1 * d19;
+            d5[i] = invd2 * d22 + invd1 * d23;
+            d6[i] = zpr * d24 + invd1 * d25;
+            d7[i] = invd2 * d20;
+            d8[i] = zpr * d26 + invd2 * d27;
+            d9[i] = zpr * d21;
+        }
+        __syncthreads();
     }
 }
 
-// precompute_xz_yz<XS, YS, ZS> (simulator3SetUp.cu:47-187) with the
-// reference launch's z blocks of 64 planes: output m of block b sums planes
-// P0 + s, s = m .. m+7 (P0 = 64 b + 1 - ZS), at the offset pair of i = 7 - (s - m),
-// weighted by INT_S_O8[max(3 - i, i - 4)] -- except that the planes s <= 6,
-// which the reference adds while priming its queues, weigh by
-// INT_S_O8[max(3 - s, s - 4)] (its loop at :120-129 uses the arriving plane's
-// index): the blocking shows in its result, and it is kept.  One thread per
-// output column and block.
+// precompute_xz_yz<XS, YS, ZS> (simulator3SetUp.cu:47-187), in the
+// reference's own form: a thread walks one 64-plane z block of its column
+// (the reference launch's blocks) and keeps the partial sums of the eight
+// outputs a plane feeds in a register queue.  Plane s of the block (the
+// block's planes start at P0 = 64 b + 1 - ZS) adds, to queue slot i (the
+// output m = s - 7 + i), the pair at x offsets X1 + i and X2 - i (X1 = -3 -
+// XS, X2 = 4 - XS; likewise in y) weighted by INT_S_O8[max(3 - i, i - 4)]
+// -- except that planes s <= 6, which the reference adds while priming its
+// queues, weigh by INT_S_O8[max(3 - s, s - 4)] (its loop at :120-129 uses
+// the arriving plane's index): the blocking shows in its result, and it is
+// kept.  Slot 0 is complete once its eighth plane has arrived.  Taps come
+// through L1.
 template <int XS, int YS, int ZS>
 __global__ void __launch_bounds__(E3X* E3Y) k_e3_precompute(const float* __restrict__ in, float* __restrict__ xz,
                                                            float* __restrict__ yz, E3Grid g)
@@ -151,21 +228,43 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_precompute(const float* __restr
     constexpr int X1 = -3 - XS, X2 = 4 - XS, Y1 = -3 - YS, Y2 = 4 - YS;
     const int b = blockIdx.z;
     const int mend = min(64, g.nz - 64 * b), p0 = 64 * b + 1 - ZS;
-    const int64_t sy = g.ldimx;
-    for (int m = 0; m < mend; ++m) {
-        float rxz = 0.0f, ryz = 0.0f;
+    const int sy = g.ldimx;
+    const int64_t sz = (int64_t)g.ldimx * g.ldimy;
+    const float* col = in + g.idx(ix, iy, p0);  // this column at the block's first plane
+    float* oxz = xz + g.idx(ix, iy, 4 + 64 * b);
+    float* oyz = yz + g.idx(ix, iy, 4 + 64 * b);
+    float qxz[8], qyz[8];
 #pragma unroll
-        for (int d = 0; d < 8; ++d) {
-            const int s = m + d, i = 7 - d;
-            const int ic = s <= 6 ? max(3 - s, s - 4) : max(3 - i, i - 4);
-            const float c = e3_int(ic);
-            const float* pl = in + g.idx(ix, iy, p0 + s);
-            rxz += c * (__ldg(pl + X1 + i) + __ldg(pl + X2 - i));
-            ryz += c * (__ldg(pl + (Y1 + i) * sy) + __ldg(pl + (Y2 - i) * sy));
+    for (int i = 0; i < 8; ++i) qxz[i] = qyz[i] = 0.0f;
+    for (int s = 0; s < mend + 7; ++s) {
+        const float* pl = col + s * sz;
+        if (s <= 6) {  // priming: one weight for the whole plane
+            const int ic = max(3 - s, s - 4);
+            const float c = ic == 0 ? e3_int(0) : ic == 1 ? e3_int(1) : ic == 2 ? e3_int(2) : e3_int(3);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                qxz[i] += c * (__ldg(pl + X1 + i) + __ldg(pl + X2 - i));
+                qyz[i] += c * (__ldg(pl + (Y1 + i) * sy) + __ldg(pl + (Y2 - i) * sy));
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float c = e3_int(max(3 - i, i - 4));
+                qxz[i] += c * (__ldg(pl + X1 + i) + __ldg(pl + X2 - i));
+                qyz[i] += c * (__ldg(pl + (Y1 + i) * sy) + __ldg(pl + (Y2 - i) * sy));
+            }
         }
-        const int64_t o = g.idx(ix, iy, 4 + 64 * b + m);
-        xz[o] = 0.5f * rxz;
-        yz[o] = 0.5f * ryz;
+        const int m = s - 7;  // the output slot 0 holds
+        if (m >= 0) {
+            oxz[m * sz] = 0.5f * qxz[0];
+            oyz[m * sz] = 0.5f * qyz[0];
+        }
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            qxz[i] = qxz[i + 1];
+            qyz[i] = qyz[i + 1];
+        }
+        qxz[7] = qyz[7] = 0.0f;
     }
 }
 
@@ -202,9 +301,11 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_splain(E3Stress a, E3Grid g)
     a.f9[i] += m(4) * yz11 + m(9) * yz22 + m(13) * yz33 + m(18) * yz12 + m(17) * yz13 + m(16) * d26;
 }
 
-// vPlainKernel (simulator3SetUp.cu:820-979): the velocity update, with the
-// z taps of f6, f8, f9 in register windows and M22 of the plane below kept
-// from the previous plane, as the reference's queues do.
+// vPlainKernel (simulator3SetUp.cu:820-979): the velocity update.  As for
+// the strains: x/y taps of f4, f5, f7, f8, f9 from shared-memory tiles of
+// each plane, z taps of f6, f8, f9 from register windows, and M22 of the
+// plane below kept from the previous plane.
+template <int V>
 __global__ void __launch_bounds__(E3X* E3Y) k_e3_vplain(float* __restrict__ f1, float* __restrict__ f2,
                                                        float* __restrict__ f3, const float* __restrict__ f4,
                                                        const float* __restrict__ f5, const float* __restrict__ f6,
@@ -212,37 +313,68 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vplain(float* __restrict__ f1, 
                                                        const float* __restrict__ f9, const float* __restrict__ M22,
                                                        const float* __restrict__ zprime, E3Grid g)
 {
-    const int ix = 4 + blockIdx.x * E3X + threadIdx.x, iy = 4 + blockIdx.y * E3Y + threadIdx.y;
-    if (ix >= 4 + g.nx || iy >= 4 + g.ny) return;
+    __shared__ __align__(16) float t4[2][E3Y][E3X + 8], t8[2][E3Y][E3X + 8];  // x taps
+    __shared__ __align__(16) float t5[2][E3Y + 8][E3X], t9[2][E3Y + 8][E3X];  // y taps
+    __shared__ __align__(16) float t7[2][E3Y + 8][E3X + 8];                   // x and y taps
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * E3X + tx;
+    const int x0 = 4 + blockIdx.x * E3X, y0 = 4 + blockIdx.y * E3Y;
+    const int ix = x0 + tx, iy = y0 + ty;
+    const bool act = ix < 4 + g.nx && iy < 4 + g.ny;
     const float invd1 = 1.01f, invd2 = 2.01f;
     const int64_t sy = g.ldimx, sz = (int64_t)g.ldimx * g.ldimy;
     const int z0 = 4 + blockIdx.z * E3ZC, z1 = min(z0 + E3ZC, 4 + g.nz);
-    float w6[9], w8[9], w9[9];  // planes iz-4 .. iz+4
-    {
+    float w6[9] = {}, w8[9] = {}, w9[9] = {};  // planes iz-4 .. iz+4
+    float m22z = 0.0f;
+    if (act) {
         const int64_t i0 = g.idx(ix, iy, z0 - 4);
-        w6[8] = w8[8] = w9[8] = 0.0f;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             w6[k + 1] = __ldg(f6 + i0 + k * sz);
             w8[k + 1] = __ldg(f8 + i0 + k * sz);
             w9[k + 1] = __ldg(f9 + i0 + k * sz);
         }
+        m22z = __ldg(M22 + g.idx(ix, iy, z0 - 1));
     }
-    float m22z = __ldg(M22 + g.idx(ix, iy, z0 - 1));
-    for (int iz = z0; iz < z1; ++iz) {
+    // planes double-buffered: plane iz+1 is copied in while plane iz is used
+    auto stage = [&](int b, int iz) {
+        const int64_t pb = (int64_t)iz * sz;
+        stage_tile_async<V>(t4[b], f4 + pb, x0 - 4, y0, g, tid);
+        stage_tile_async<V>(t8[b], f8 + pb, x0 - 4, y0, g, tid);
+        stage_tile_async<V>(t5[b], f5 + pb, x0, y0 - 4, g, tid);
+        stage_tile_async<V>(t9[b], f9 + pb, x0, y0 - 4, g, tid);
+        stage_tile_async<V>(t7[b], f7 + pb, x0 - 4, y0 - 4, g, tid);
+        __pipeline_commit();
+    };
+    if (z0 < z1) stage(0, z0);
+    for (int iz = z0, b = 0; iz < z1; ++iz, b ^= 1) {
         const int64_t i = g.idx(ix, iy, iz);
-        zshift(w6, f6, i + 4 * sz);
-        zshift(w8, f8, i + 4 * sz);
-        zshift(w9, f9, i + 4 * sz);
-        const float d10 = drv8<true>(f4 + i, 1), d11 = drv8<true>(f5 + i, sy), d12 = zdrv(w6, true);
-        const float d13 = drv8<false>(f7 + i, 1), d14 = drv8<false>(f7 + i, sy), d15 = zdrv(w8, false);
-        const float d16 = drv8<false>(f8 + i, 1), d17 = drv8<false>(f9 + i, sy), d18 = zdrv(w9, false);
-        const float zpr = __ldg(zprime + iz);
-        const float m22c = __ldg(M22 + i);
-        f1[i] += (2.0f * __ldg(M22 + i - 1)) * (d10 * invd1 + d14 * invd2 + d15 * zpr);
-        f2[i] += (2.0f * __ldg(M22 + i - sy)) * (d13 * invd1 + d11 * invd2 + d18 * zpr);
-        f3[i] += (2.0f * m22z) * (d16 * invd1 + d17 * invd2 + d12 * zpr);
-        m22z = m22c;
+        if (iz + 1 < z1) stage(b ^ 1, iz + 1);
+        float m22c = 0.0f, mx = 0.0f, my = 0.0f;
+        if (act) {
+            zshift(w6, f6, i + 4 * sz);
+            zshift(w8, f8, i + 4 * sz);
+            zshift(w9, f9, i + 4 * sz);
+            m22c = __ldg(M22 + i);
+            mx = __ldg(M22 + i - 1);
+            my = __ldg(M22 + i - sy);
+        }
+        __pipeline_wait_prior(iz + 1 < z1 ? 1 : 0);
+        __syncthreads();
+        if (act) {
+            const float d10 = drv8s<true>(&t4[b][ty][tx + 4], 1), d11 = drv8s<true>(&t5[b][ty + 4][tx], E3X);
+            const float d12 = zdrv(w6, true);
+            const float d13 = drv8s<false>(&t7[b][ty + 4][tx + 4], 1);
+            const float d14 = drv8s<false>(&t7[b][ty + 4][tx + 4], E3X + 8);
+            const float d15 = zdrv(w8, false);
+            const float d16 = drv8s<false>(&t8[b][ty][tx + 4], 1), d17 = drv8s<false>(&t9[b][ty + 4][tx], E3X);
+            const float d18 = zdrv(w9, false);
+            const float zpr = __ldg(zprime + iz);
+            f1[i] += (2.0f * mx) * (d10 * invd1 + d14 * invd2 + d15 * zpr);
+            f2[i] += (2.0f * my) * (d13 * invd1 + d11 * invd2 + d18 * zpr);
+            f3[i] += (2.0f * m22z) * (d16 * invd1 + d17 * invd2 + d12 * zpr);
+            m22z = m22c;
+        }
+        __syncthreads();
     }
 }
 
@@ -319,6 +451,15 @@ __global__ void k_e3_init_model(E3Model a, int nx, int ldimx, int ldimy, int ldi
 
 inline cudaStream_t S(tti_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// 16-byte staging copies need rows of whole 4-float chunks and aligned volumes.
+bool vec4_ok(int ldimx, std::initializer_list<const float*> vols)
+{
+    if (ldimx % 4) return false;
+    for (const float* v : vols)
+        if (reinterpret_cast<uintptr_t>(v) % 16) return false;
+    return true;
+}
+
 bool e3_grid_ok(int nx, int ny, int nz, int ldimx, int ldimy)
 {
     return nx > 0 && ny > 0 && nz > 0 && ldimx >= nx + 8 && ldimy >= ny + 8;
@@ -339,7 +480,12 @@ int tti_e3_launch_vgplain(const float* f1, const float* f2, const float* f3, flo
         !zprime)
         return TTI_EINVAL;
     const E3Grid g{nx, ny, nz, ldimx, ldimy};
-    k_e3_vgplain<<<e3_blocks(g, E3ZC), dim3(E3X, E3Y), 0, S(stream)>>>(f1, f2, f3, d4, d5, d6, d7, d8, d9, zprime, g);
+    if (vec4_ok(ldimx, {f1, f2, f3}))
+        k_e3_vgplain<4><<<e3_blocks(g, E3ZC), dim3(E3X, E3Y), 0, S(stream)>>>(f1, f2, f3, d4, d5, d6, d7, d8, d9,
+                                                                              zprime, g);
+    else
+        k_e3_vgplain<1><<<e3_blocks(g, E3ZC), dim3(E3X, E3Y), 0, S(stream)>>>(f1, f2, f3, d4, d5, d6, d7, d8, d9,
+                                                                              zprime, g);
     return launch_status();
 }
 
@@ -394,8 +540,12 @@ int tti_e3_launch_vplain(float* f1, float* f2, float* f3, const float* f4, const
         !M22 || !zprime)
         return TTI_EINVAL;
     const E3Grid g{nx, ny, nz, ldimx, ldimy};
-    k_e3_vplain<<<e3_blocks(g, E3ZC), dim3(E3X, E3Y), 0, S(stream)>>>(f1, f2, f3, f4, f5, f6, f7, f8, f9, M22, zprime,
-                                                                      g);
+    if (vec4_ok(ldimx, {f4, f5, f7, f8, f9}))
+        k_e3_vplain<4><<<e3_blocks(g, E3ZC), dim3(E3X, E3Y), 0, S(stream)>>>(f1, f2, f3, f4, f5, f6, f7, f8, f9, M22,
+                                                                             zprime, g);
+    else
+        k_e3_vplain<1><<<e3_blocks(g, E3ZC), dim3(E3X, E3Y), 0, S(stream)>>>(f1, f2, f3, f4, f5, f6, f7, f8, f9, M22,
+                                                                             zprime, g);
     return launch_status();
 }
 

@@ -154,3 +154,38 @@ def test_composed_schedule_against_the_oracle():
     assert np.isfinite(g2).all()
     assert maxerr(g2, want["g2"][inner]) < 1e-4
     assert sim.launches == 3 * 8 + 3 * 7 + 3 * 2
+
+
+class OddLayout:
+    """A halo'd layout whose rows are not a multiple of four floats (the
+    launchers then stage their tiles with 4-byte copies)."""
+
+    def __init__(self, nx, ny, nz):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.ldimx, self.ldimy, self.ldimz = nx + 9, ny + 8, nz + 8
+        self.shape = (self.ldimz, self.ldimy, self.ldimx)
+
+    def zeros(self):
+        return np.zeros(self.shape, np.float32)
+
+
+def test_velocity_kernels_on_rows_of_odd_length():
+    from miniappsforhpe_b200 import elastic as E
+
+    lay = OddLayout(40, 20, 70)
+    rng = np.random.default_rng(14)
+    v, s, (M22,) = vols(3, rng, lay), vols(6, rng, lay), vols(1, rng, lay)
+    zp = np.cos(6 * np.arange(lay.ldimz, dtype=np.float32)).astype(np.float32)
+    e = ElasticOracle()
+    d = [lay.zeros() for _ in range(6)]
+    e.vgplain(lay, *v, d, zp)
+    v_o = [x.copy() for x in v]
+    e.vplain(lay, v_o, s, M22, zp)
+    gv, gd, gz = dev(v), dev([lay.zeros() for _ in range(6)]), torch.from_numpy(zp).cuda()
+    E.launch_vgplain(*gv, *gd, gz, lay.nx, lay.ny, lay.nz, lay.ldimx, lay.ldimy)
+    E.launch_vplain(*gv, *dev(s), torch.from_numpy(M22).cuda(), gz, lay.nx, lay.ny, lay.nz, lay.ldimx, lay.ldimy)
+    torch.cuda.synchronize()
+    for a, b in zip(host(gd), d):
+        assert maxerr(a, b) < 1e-5
+    for a, b in zip(host(gv), v_o):
+        assert maxerr(a, b) < 1e-5
