@@ -189,3 +189,22 @@ def test_velocity_kernels_on_rows_of_odd_length():
         assert maxerr(a, b) < 1e-5
     for a, b in zip(host(gv), v_o):
         assert maxerr(a, b) < 1e-5
+
+
+def test_stress_update_on_rows_of_odd_length():
+    from miniappsforhpe_b200 import elastic as E
+
+    lay = OddLayout(40, 20, 70)
+    rng = np.random.default_rng(15)
+    s, M, d = vols(6, rng, lay), vols(21, rng, lay), vols(6, rng, lay)
+    pre = [lay.zeros() for _ in range(12)]
+    gs, gpre = dev(s), dev(pre)
+    s_o = [x.copy() for x in s]
+    ElasticOracle().splain(lay, s_o, M, d, pre)
+    E.launch_splain(*gs, dev(M), *dev(d), gpre, lay.nx, lay.ny, lay.nz, lay.ldimx, lay.ldimy)
+    torch.cuda.synchronize()
+    I = (slice(4, 4 + lay.nz), slice(4, 4 + lay.ny), slice(4, 4 + lay.nx))
+    for a, b in zip(host(gpre), pre):
+        assert maxerr(a[I], b[I]) < 1e-5
+    for a, b in zip(host(gs), s_o):
+        assert maxerr(a, b) < 1e-5
