@@ -457,12 +457,17 @@ def run_ours(args):
         b_step = B_VTI if vti else (B_FWD if kind == "forward" else B_ADJ)
     alg_bytes = b_step * npts
     achieved = alg_bytes / per_launch_s / 1e9 if kn else None
+    # DRAM bytes per launch from the committed ncu capture at this run's work
+    # split (the traffic depends on it: L2 keeps the halos neighbouring
+    # columns share only when their CTAs run side by side)
     tkey = f"{'type1_' if t1 else ''}{kind}"
-    tr = ncu_traffic()
-    traffic = tr.get(f"{tkey}_dram_bytes_per_launch_{nx}x{ny}x{nz}")
+    sp = (tuned or {}).get(tkey)
+    split = [sp["bz"], sp.get("ztop", 0)] if isinstance(sp, dict) else None
+    traffic = (ncu_traffic().get(f"{tkey}_dram_bytes_per_launch_{nx}x{ny}x{nz}_{split[0]}x{split[1]}")
+               if split else None)
     roofline = {"kernel": f"fused {'type1 ' if t1 else ''}{kind} step", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                "traffic": traffic, "traffic_split": tr.get(f"{tkey}_split_{nx}x{ny}x{nz}"),
+                "traffic": traffic, "traffic_split": split,
                 "alg_bytes_per_launch": alg_bytes,
                 "avg_launch_ms": per_launch_s * 1e3, "launches": kn}
     passes = {k: {"total_ms": v[0] / args.steps, "launches_per_shot": v[1] / args.steps}
