@@ -325,9 +325,10 @@ int tti_selfcheck_bounded_wait(double seconds, tti_stream_t stream);
  * on grids with fewer tile columns than SMs, top/bottom splits as for
  * tti_tune_set_split around the balance point of the tops) of the fused
  * forward, adjoint and (with a snapshot store) imaging kernels on this
- * simulator's volumes, reps launches each, times the three fastest again
- * with more launches and records the fastest (a top/bottom split within 1 %
- * of it is taken instead: same speed, about half the DRAM traffic) for this
+ * simulator's volumes, reps launches each, times the three fastest (and the
+ * fastest top/bottom split, if within 3 %) again with more launches and
+ * records the fastest (a top/bottom split within 1 % of it is taken
+ * instead: same speed, about half the DRAM traffic) for this
  * grid on the current device; later launches on any simulator of the same
  * grid use it.  Needs fused = 1 and a model.  Wavefield and image contents
  * afterwards are unspecified (forward and adjoint start from zero).  The

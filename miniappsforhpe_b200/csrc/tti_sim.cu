@@ -1809,6 +1809,15 @@ int tti_sim_autotune(tti_sim* s, int reps, tti_tune_report* out)
         std::vector<Split> finalists;
         for (size_t k = 0; k < timed.size() && finalists.size() < 3; ++k) finalists.push_back(timed[k].second);
         if (std::find(finalists.begin(), finalists.end(), modelled) == finalists.end()) finalists.push_back(modelled);
+        // the fastest top/bottom candidate too, when it is within 3 % on the
+        // first pass (the tie-break below can only prefer a finalist)
+        for (const auto& t : timed)
+            if (t.second.ztop > 0) {
+                if (t.first <= 1.03f * timed.front().first &&
+                    std::find(finalists.begin(), finalists.end(), t.second) == finalists.end())
+                    finalists.push_back(t.second);
+                break;
+            }
         std::vector<std::pair<float, Split>> fin;
         for (const Split& sp : finalists) {
             float ms = 0;
