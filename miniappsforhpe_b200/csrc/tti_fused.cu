@@ -1096,9 +1096,16 @@ constexpr int IMG_PF = 2;
 __host__ __device__ constexpr size_t img_p(size_t elt) { return (size_t)PH * PW * elt; }
 constexpr size_t IMG_A = (size_t)IH * IW * sizeof(float);
 constexpr size_t IMG_A4 = (size_t)IH * IW * sizeof(float4);
-__host__ __device__ constexpr size_t img_stage(size_t elt, bool tti)
+// then the point-wise values of the plane's output columns (TX x TY, no
+// halo): the stored pdot, qdot (storage type), the adjoint pdot, qdot and the
+// Vp image at this plane, and the density gradient at plane L-7 (float)
+__host__ __device__ constexpr size_t img_halo_part(size_t elt, bool tti)
 {
     return 2 * img_p(elt) + 2 * IMG_A + IMG_A4 + (tti ? IMG_A4 : IMG_A);
+}
+__host__ __device__ constexpr size_t img_stage(size_t elt, bool tti)
+{
+    return img_halo_part(elt, tti) + (size_t)TX * TY * (2 * elt + 4 * sizeof(float));
 }
 constexpr size_t IMG_T1 = (size_t)2 * TY * IW * sizeof(float);  // x-type tiles: rows y0.., cols x0-4..
 constexpr size_t IMG_T2 = (size_t)2 * IH * TX * sizeof(float);  // y-type tiles: rows y0-4.., cols x0..
@@ -1112,6 +1119,9 @@ struct ImgMaps {
     CUtensorMap p, q;   // adjoint p, q: box IW x IH
     CUtensorMap ma;     // 4D (4, x, y, z), box 4 x IW x IH
     CUtensorMap mb;     // TTI: like ma; VTI: irho, box IW x IH
+    CUtensorMap snapc;  // the store again, box TX x TY
+    CUtensorMap f3, f4; // adjoint pdot, qdot: box TX x TY
+    CUtensorMap gv, gr; // the dense images (nx, ny, nz, 1): box TX x TY
 };
 
 
@@ -1121,6 +1131,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
     extern __shared__ __align__(1024) unsigned char smem[];
     constexpr size_t IMG_P = img_p(sizeof(T));
     constexpr size_t IMG_STAGE = img_stage(sizeof(T), TTI);
+    constexpr size_t IMG_CT = (size_t)TX * TY * sizeof(T);  // one point-wise tile of the storage type
     unsigned char* stage = smem;
     unsigned char* sp = smem + IMG_NSTAGE * IMG_STAGE;
     // x-type and y-type tiles, one float4 per cell: forward derivative of
@@ -1191,6 +1202,16 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             tma_load_4d(adst + 2 * IMG_A + IMG_A4, &tm.mb, 0, x0 - 4, y0 - 4, z, &bars[s]);
         else
             tma_load_3d(adst + 2 * IMG_A + IMG_A4, &tm.mb, x0 - 4, y0 - 4, z, &bars[s]);
+        // point-wise values (zero-filled where z or z-LAG is outside the grid)
+        unsigned char* cdst = dst + img_halo_part(sizeof(T), TTI);
+        const int zc = z - L.izbeg;
+        tma_load_4d(cdst, &tm.snapc, xd0, yd0, zc, 4 * a.slot, &bars[s]);
+        tma_load_4d(cdst + IMG_CT, &tm.snapc, xd0, yd0, zc, 4 * a.slot + 1, &bars[s]);
+        float* cf = reinterpret_cast<float*>(cdst + 2 * IMG_CT);
+        tma_load_3d(cf, &tm.f3, x0, y0, z, &bars[s]);
+        tma_load_3d(cf + TX * TY, &tm.f4, x0, y0, z, &bars[s]);
+        tma_load_4d(cf + 2 * TX * TY, &tm.gv, xd0, yd0, zc, 0, &bars[s]);
+        tma_load_4d(cf + 3 * TX * TY, &tm.gr, xd0, yd0, zc - LAG, 0, &bars[s]);
     };
     if (tid == 0)
         for (int t = 0; t < IMG_PF && t < ntot; ++t) issue(t);
@@ -1219,24 +1240,27 @@ __global__ void __launch_bounds__(NT, 1) k_fused_image(const __grid_constant__ I
             issue(t + IMG_PF);
         }
         const int Lz = zs - LAG + t;
-        // point-wise global values of this iteration, loaded ahead of their use
         const bool vp_here = owner && Lz >= zs && Lz <= ze;
         const bool rho_here = owner && (Lz - LAG) >= zs;
         const int64_t dvp = ((int64_t)(Lz - L.izbeg) * ny + (y - L.iybeg)) * nx + (x - L.ixbeg);
         const int64_t drho = dvp - (int64_t)LAG * nx * ny;
-        float ps3 = 0.0f, ps4 = 0.0f, pa3 = 0.0f, pa4 = 0.0f, pgv = 0.0f, pgr = 0.0f;
-        if (vp_here) {
-            const int64_t gi = L.idx(x, y, Lz);
-            ps3 = to_f32(static_cast<const T*>(a.snap3)[dvp]) * us3;
-            ps4 = to_f32(static_cast<const T*>(a.snap4)[dvp]) * us4;
-            pa3 = __ldg(a.f3 + gi);
-            pa4 = __ldg(a.f4 + gi);
-            pgv = a.gvp[dvp];
-        }
-        if (rho_here) pgr = a.grho[drho];
         g_wait = gbase + t;
         mbar_wait(&bars[s], phase, a.err, dead);
         unsigned char* st = stage + (size_t)s * IMG_STAGE;
+        // point-wise values of this column, staged with the plane
+        float ps3, ps4, pa3, pa4, pgv, pgr;
+        {
+            const unsigned char* cst = st + img_halo_part(sizeof(T), TTI);
+            const T* S3 = reinterpret_cast<const T*>(cst);
+            const float* CF = reinterpret_cast<const float*>(cst + 2 * IMG_CT);
+            const int kc0 = ty * TX + tx;
+            ps3 = to_f32(S3[kc0]) * us3;
+            ps4 = to_f32(S3[TX * TY + kc0]) * us4;
+            pa3 = CF[kc0];
+            pa4 = CF[TX * TY + kc0];
+            pgv = CF[2 * TX * TY + kc0];
+            pgr = CF[3 * TX * TY + kc0];
+        }
         const bool mirrored = a.fs && Lz < L.izbeg;
         if (mirrored) {  // block-uniform
             T* pt = reinterpret_cast<T*>(st);
@@ -2478,6 +2502,11 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
         !get_map4(&tm.ma, s.m.ma, L, IW, IH))
         return TTI_ELAUNCH;
     if (tti ? !get_map4(&tm.mb, s.m.mb, L, IW, IH) : !get_map(&tm.mb, s.m.irho, L, IW, IH)) return TTI_ELAUNCH;
+    if (!get_map(&tm.f3, s.adj3, L, TX, TY) || !get_map(&tm.f4, s.adj4, L, TX, TY)) return TTI_ELAUNCH;
+    if (!make_store_map(&tm.snapc, s.store, s.snap_prec, L.nx(), L.ny(), L.nz(), 4 * s.nsnap, TX, TY) ||
+        !make_store_map(&tm.gv, s.grad_vp, SNAP_F32, L.nx(), L.ny(), L.nz(), 1, TX, TY) ||
+        !make_store_map(&tm.gr, s.grad_rho, SNAP_F32, L.nx(), L.ny(), L.nz(), 1, TX, TY))
+        return TTI_ELAUNCH;
     ImgParams a{};
     a.f3 = s.adj3;
     a.f4 = s.adj4;
