@@ -1072,8 +1072,6 @@ __global__ void __launch_bounds__(NT, 1) k_fused_adjoint(const __grid_constant__
 // interior volumes, free-surface halo re-derived by mirroring); the adjoint
 // temporaries adj_a = rho*(s1 + ra^2 h1) come from the current adjoint p/q.
 struct ImgParams {
-    const float *f3, *f4;
-    const void *snap3, *snap4;  // dense pdot/qdot of this snapshot (storage type)
     const float* snap_scale;    // the 4 multipliers the slot was stored with
     float *gvp, *grho;           // dense images
     Layout L;
@@ -2508,12 +2506,6 @@ int launch_fused_image(const Layout& L, const ImageArgs& s, cudaStream_t st)
         !make_store_map(&tm.gr, s.grad_rho, SNAP_F32, L.nx(), L.ny(), L.nz(), 1, TX, TY))
         return TTI_ELAUNCH;
     ImgParams a{};
-    a.f3 = s.adj3;
-    a.f4 = s.adj4;
-    const int64_t nin = (int64_t)L.nx() * L.ny() * L.nz();
-    const size_t elt = snap_elt_bytes(s.snap_prec);
-    a.snap3 = static_cast<const unsigned char*>(s.store) + (size_t)s.slot * 4 * nin * elt;
-    a.snap4 = static_cast<const unsigned char*>(a.snap3) + (size_t)nin * elt;
     a.snap_scale = s.snap_prec == SNAP_F32 ? nullptr : s.snap_scale;
     a.gvp = s.grad_vp;
     a.grho = s.grad_rho;
