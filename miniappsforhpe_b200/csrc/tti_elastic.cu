@@ -319,7 +319,9 @@ __global__ void __launch_bounds__(E3X* E3Y, 5) k_e3_splain(E3Stress a, E3Grid g)
 // vPlainKernel (simulator3SetUp.cu:820-979): the velocity update.  As for
 // the strains: x/y taps of f4, f5, f7, f8, f9 from shared-memory tiles of
 // each plane, z taps of f6, f8, f9 from register windows, and M22 of the
-// plane below kept from the previous plane.
+// plane below kept from the previous plane; M22 (with the row above and
+// the columns left of the tile) and the three velocities it updates come
+// through shared tiles of the plane too.
 template <int V>
 __global__ void __launch_bounds__(E3X* E3Y) k_e3_vplain(float* __restrict__ f1, float* __restrict__ f2,
                                                        float* __restrict__ f3, const float* __restrict__ f4,
@@ -331,6 +333,8 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vplain(float* __restrict__ f1, 
     __shared__ __align__(16) float t4[2][E3Y][E3X + 8], t8[2][E3Y][E3X + 8];  // x taps
     __shared__ __align__(16) float t5[2][E3Y + 8][E3X], t9[2][E3Y + 8][E3X];  // y taps
     __shared__ __align__(16) float t7[2][E3Y + 8][E3X + 8];                   // x and y taps
+    __shared__ __align__(16) float tm[2][E3Y + 1][E3X + 4];                   // M22: rows y0-1.., cols x0-4..
+    __shared__ __align__(16) float tv[2][3][E3Y][E3X];                        // f1, f2, f3
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * E3X + tx;
     const int x0 = 4 + blockIdx.x * E3X, y0 = 4 + blockIdx.y * E3Y;
     const int ix = x0 + tx, iy = y0 + ty;
@@ -358,24 +362,25 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vplain(float* __restrict__ f1, 
         stage_tile_async<V>(t5[b], f5 + pb, x0, y0 - 4, g, tid);
         stage_tile_async<V>(t9[b], f9 + pb, x0, y0 - 4, g, tid);
         stage_tile_async<V>(t7[b], f7 + pb, x0 - 4, y0 - 4, g, tid);
+        stage_tile_async<V>(tm[b], M22 + pb, x0 - 4, y0 - 1, g, tid);
+        stage_tile_async<V>(tv[b][0], f1 + pb, x0, y0, g, tid);
+        stage_tile_async<V>(tv[b][1], f2 + pb, x0, y0, g, tid);
+        stage_tile_async<V>(tv[b][2], f3 + pb, x0, y0, g, tid);
         __pipeline_commit();
     };
     if (z0 < z1) stage(0, z0);
     for (int iz = z0, b = 0; iz < z1; ++iz, b ^= 1) {
         const int64_t i = g.idx(ix, iy, iz);
         if (iz + 1 < z1) stage(b ^ 1, iz + 1);
-        float m22c = 0.0f, mx = 0.0f, my = 0.0f;
         if (act) {
             zshift(w6, f6, i + 4 * sz);
             zshift(w8, f8, i + 4 * sz);
             zshift(w9, f9, i + 4 * sz);
-            m22c = __ldg(M22 + i);
-            mx = __ldg(M22 + i - 1);
-            my = __ldg(M22 + i - sy);
         }
         __pipeline_wait_prior(iz + 1 < z1 ? 1 : 0);
         __syncthreads();
         if (act) {
+            const float m22c = tm[b][ty + 1][tx + 4], mx = tm[b][ty + 1][tx + 3], my = tm[b][ty][tx + 4];
             const float d10 = drv8s<true>(&t4[b][ty][tx + 4], 1), d11 = drv8s<true>(&t5[b][ty + 4][tx], E3X);
             const float d12 = zdrv(w6, true);
             const float d13 = drv8s<false>(&t7[b][ty + 4][tx + 4], 1);
@@ -384,9 +389,9 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vplain(float* __restrict__ f1, 
             const float d16 = drv8s<false>(&t8[b][ty][tx + 4], 1), d17 = drv8s<false>(&t9[b][ty + 4][tx], E3X);
             const float d18 = zdrv(w9, false);
             const float zpr = __ldg(zprime + iz);
-            f1[i] += (2.0f * mx) * (d10 * invd1 + d14 * invd2 + d15 * zpr);
-            f2[i] += (2.0f * my) * (d13 * invd1 + d11 * invd2 + d18 * zpr);
-            f3[i] += (2.0f * m22z) * (d16 * invd1 + d17 * invd2 + d12 * zpr);
+            f1[i] = tv[b][0][ty][tx] + (2.0f * mx) * (d10 * invd1 + d14 * invd2 + d15 * zpr);
+            f2[i] = tv[b][1][ty][tx] + (2.0f * my) * (d13 * invd1 + d11 * invd2 + d18 * zpr);
+            f3[i] = tv[b][2][ty][tx] + (2.0f * m22z) * (d16 * invd1 + d17 * invd2 + d12 * zpr);
             m22z = m22c;
         }
         __syncthreads();
@@ -564,7 +569,7 @@ int tti_e3_launch_vplain(float* f1, float* f2, float* f3, const float* f4, const
         !M22 || !zprime)
         return TTI_EINVAL;
     const E3Grid g{nx, ny, nz, ldimx, ldimy};
-    if (vec4_ok(ldimx, {f4, f5, f7, f8, f9}))
+    if (vec4_ok(ldimx, {f1, f2, f3, f4, f5, f7, f8, f9, M22}))
         k_e3_vplain<4><<<e3_blocks(g, E3ZC), dim3(E3X, E3Y), 0, S(stream)>>>(f1, f2, f3, f4, f5, f6, f7, f8, f9, M22,
                                                                              zprime, g);
     else
