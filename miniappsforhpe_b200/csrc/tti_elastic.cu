@@ -84,12 +84,12 @@ __device__ __forceinline__ float zdrv(const float (&w)[9], bool shift)
     return d;
 }
 
-// Shift a 9-plane window one plane down and take plane k+4 of the column.
-__device__ __forceinline__ void zshift(float (&w)[9], const float* __restrict__ p, int64_t next)
+// Shift a 9-plane window one plane down and append the new plane's value.
+__device__ __forceinline__ void zpush(float (&w)[9], float v)
 {
 #pragma unroll
     for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
-    w[8] = __ldg(p + next);
+    w[8] = v;
 }
 
 // drv1_8 on a shared-memory tile (stride s between taps).
@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vgplain(const float* __restrict
                                                         E3Grid g)
 {
     __shared__ __align__(16) float t1[2][E3Y + 8][E3X + 8], t2[2][E3Y + 8][E3X + 8], t3[2][E3Y + 8][E3X + 8];
+    __shared__ __align__(16) float tw[2][3][E3Y][E3X];  // f1, f2, f3 of plane iz+4 (the windows' new plane)
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * E3X + tx;
     const int x0 = 4 + blockIdx.x * E3X, y0 = 4 + blockIdx.y * E3Y;
     const int ix = x0 + tx, iy = y0 + ty;
@@ -174,20 +175,22 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vgplain(const float* __restrict
         stage_tile_async<V>(t1[b], f1 + pb, x0 - 4, y0 - 4, g, tid);
         stage_tile_async<V>(t2[b], f2 + pb, x0 - 4, y0 - 4, g, tid);
         stage_tile_async<V>(t3[b], f3 + pb, x0 - 4, y0 - 4, g, tid);
+        const int64_t pw = pb + 4 * sz;
+        stage_tile_async<V>(tw[b][0], f1 + pw, x0, y0, g, tid);
+        stage_tile_async<V>(tw[b][1], f2 + pw, x0, y0, g, tid);
+        stage_tile_async<V>(tw[b][2], f3 + pw, x0, y0, g, tid);
         __pipeline_commit();
     };
     if (z0 < z1) stage(0, z0);
     for (int iz = z0, b = 0; iz < z1; ++iz, b ^= 1) {
         const int64_t i = g.idx(ix, iy, iz);
         if (iz + 1 < z1) stage(b ^ 1, iz + 1);
-        if (act) {
-            zshift(w1, f1, i + 4 * sz);
-            zshift(w2, f2, i + 4 * sz);
-            zshift(w3, f3, i + 4 * sz);
-        }
         __pipeline_wait_prior(iz + 1 < z1 ? 1 : 0);
         __syncthreads();
         if (act) {
+            zpush(w1, tw[b][0][ty][tx]);
+            zpush(w2, tw[b][1][ty][tx]);
+            zpush(w3, tw[b][2][ty][tx]);
             constexpr int S = E3X + 8;
             const float* c1 = &t1[b][ty + 4][tx + 4];
             const float* c2 = &t2[b][ty + 4][tx + 4];
@@ -288,32 +291,92 @@ struct E3Stress {
     const float* p[12];                             // f10 .. f21
 };
 
-// sPlainKernel (simulator3SetUp.cu:980-1103): the stress update.  It waits
-// on its 45 streamed loads per cell, so it is held to 48 registers for five
-// blocks per SM (5 % faster than at 58 registers, 12 bytes spilled).
-__global__ void __launch_bounds__(E3X* E3Y, 5) k_e3_splain(E3Stress a, E3Grid g)
+// mixed_XY on a shared-memory tile (row stride sy).
+template <bool XS, bool YS>
+__device__ __forceinline__ float mixed8s(const float* p, int sy)
 {
-    const int ix = 4 + blockIdx.x * E3X + threadIdx.x, iy = 4 + blockIdx.y * E3Y + threadIdx.y;
-    if (ix >= 4 + g.nx || iy >= 4 + g.ny) return;
-    const int iz = 4 + blockIdx.z;
-    const int64_t i = g.idx(ix, iy, iz), sy = g.ldimx;
-    auto m = [&](int k) { return __ldg(a.M[k - 1] + i); };
-    auto p = [&](int k) { return __ldg(a.p[k - 10] + i); };  // f10 .. f21
-    const float d19 = __ldg(a.e11 + i), d20 = __ldg(a.e22 + i), d21 = __ldg(a.e33 + i);
-    const float d22 = __ldg(a.e12 + i), d24 = __ldg(a.e13 + i), d26 = __ldg(a.e23 + i);
-    const float xx12 = mixed8<false, false>(a.e12 + i, sy), xx13 = p(14), xx23 = p(19);
-    a.f4[i] += m(1) * d19 + m(2) * d20 + m(3) * d21 + m(6) * xx12 + m(5) * xx13 + m(4) * xx23;
-    a.f5[i] += m(2) * d19 + m(7) * d20 + m(8) * d21 + m(11) * xx12 + m(10) * xx13 + m(9) * xx23;
-    a.f6[i] += m(3) * d19 + m(8) * d20 + m(12) * d21 + m(15) * xx12 + m(14) * xx13 + m(13) * xx23;
-    const float xy11 = mixed8<true, true>(a.e11 + i, sy), xy22 = mixed8<true, true>(a.e22 + i, sy);
-    const float xy33 = mixed8<true, true>(a.e33 + i, sy), xy13 = p(15), xy23 = p(18);
-    a.f7[i] += m(6) * xy11 + m(11) * xy22 + m(15) * xy33 + m(20) * xy13 + m(18) * xy23 + m(21) * d22;
-    const float xz11 = p(10), xz22 = p(16), xz33 = p(20), xz12 = p(13);
-    const float xz23 = mixed8<true, false>(a.e23 + i, sy);
-    a.f8[i] += m(5) * xz11 + m(10) * xz22 + m(14) * xz33 + m(20) * xz12 + m(17) * xz23 + m(19) * d24;
-    const float yz11 = p(11), yz22 = p(17), yz33 = p(21), yz12 = p(12);
-    const float yz13 = mixed8<false, true>(a.e13 + i, sy);
-    a.f9[i] += m(4) * yz11 + m(9) * yz22 + m(13) * yz33 + m(18) * yz12 + m(17) * yz13 + m(16) * d26;
+    constexpr int xs = XS ? -1 : 0, ys = YS ? -1 : 0;
+    float d = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        d += e3_int(i) * (p[(ys + i + 1) * sy + xs + i + 1] + p[(ys + i + 1) * sy + xs - i] +
+                          p[(ys - i) * sy + xs + i + 1] + p[(ys - i) * sy + xs - i]);
+    return 0.5f * d;
+}
+
+// sPlainKernel (simulator3SetUp.cu:980-1103): the stress update.  A block
+// walks E3ZS planes of a 32x8 column tile; every array it reads comes
+// through shared memory, double-buffered and filled by asynchronous copies
+// while the previous plane is used: the 21 Cij, the 12 z-mixed volumes and
+// the 6 stresses it updates as 32x8 tiles, the 6 strains as tiles with a
+// halo of 4 for their mixed x/y taps.
+constexpr int E3ZS = 16;                         // planes per block
+constexpr int E3C = E3X * E3Y;                   // a center tile
+constexpr int E3H = (E3Y + 8) * (E3X + 8);       // a tile with a halo of 4
+constexpr int E3SBUF = 39 * E3C + 6 * E3H;       // floats per buffer
+constexpr size_t E3S_SMEM = 2 * E3SBUF * sizeof(float);
+
+template <int V>
+__global__ void __launch_bounds__(E3X* E3Y, 2) k_e3_splain(E3Stress a, E3Grid g)
+{
+    extern __shared__ __align__(16) float e3s[];
+    using Ctile = float[E3Y][E3X];
+    using Htile = float[E3Y + 8][E3X + 8];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * E3X + tx;
+    const int x0 = 4 + blockIdx.x * E3X, y0 = 4 + blockIdx.y * E3Y;
+    const int ix = x0 + tx, iy = y0 + ty;
+    const bool act = ix < 4 + g.nx && iy < 4 + g.ny;
+    const int64_t sz = (int64_t)g.ldimx * g.ldimy;
+    const int z0 = 4 + blockIdx.z * E3ZS, z1 = min(z0 + E3ZS, 4 + g.nz);
+    const float* const ein[6] = {a.e11, a.e12, a.e13, a.e22, a.e23, a.e33};
+    float* const fout[6] = {a.f4, a.f5, a.f6, a.f7, a.f8, a.f9};
+    auto ctile = [&](int b, int k) -> Ctile& { return *reinterpret_cast<Ctile*>(e3s + b * E3SBUF + k * E3C); };
+    auto htile = [&](int b, int k) -> Htile& {
+        return *reinterpret_cast<Htile*>(e3s + b * E3SBUF + 39 * E3C + k * E3H);
+    };
+    // tiles 0..20: M1..M21, 21..32: f10..f21, 33..38: f4..f9; halo tiles: e11, e12, e13, e22, e23, e33
+    auto stage = [&](int b, int iz) {
+        const int64_t pb = (int64_t)iz * sz;
+        for (int k = 0; k < 21; ++k) stage_tile_async<V>(ctile(b, k), a.M[k] + pb, x0, y0, g, tid);
+        for (int k = 0; k < 12; ++k) stage_tile_async<V>(ctile(b, 21 + k), a.p[k] + pb, x0, y0, g, tid);
+        for (int k = 0; k < 6; ++k) stage_tile_async<V>(ctile(b, 33 + k), fout[k] + pb, x0, y0, g, tid);
+        for (int k = 0; k < 6; ++k) stage_tile_async<V>(htile(b, k), ein[k] + pb, x0 - 4, y0 - 4, g, tid);
+        __pipeline_commit();
+    };
+    if (z0 < z1) stage(0, z0);
+    for (int iz = z0, b = 0; iz < z1; ++iz, b ^= 1) {
+        if (iz + 1 < z1) stage(b ^ 1, iz + 1);
+        __pipeline_wait_prior(iz + 1 < z1 ? 1 : 0);
+        __syncthreads();
+        if (act) {
+            const int64_t i = g.idx(ix, iy, iz);
+            constexpr int S = E3X + 8;
+            auto m = [&](int k) { return ctile(b, k - 1)[ty][tx]; };
+            auto p = [&](int k) { return ctile(b, 21 + k - 10)[ty][tx]; };  // f10 .. f21
+            auto f = [&](int k) { return ctile(b, 33 + k)[ty][tx]; };       // f4 .. f9
+            const float* c11 = &htile(b, 0)[ty + 4][tx + 4];
+            const float* c12 = &htile(b, 1)[ty + 4][tx + 4];
+            const float* c13 = &htile(b, 2)[ty + 4][tx + 4];
+            const float* c22 = &htile(b, 3)[ty + 4][tx + 4];
+            const float* c23 = &htile(b, 4)[ty + 4][tx + 4];
+            const float* c33 = &htile(b, 5)[ty + 4][tx + 4];
+            const float d19 = *c11, d20 = *c22, d21 = *c33, d22 = *c12, d24 = *c13, d26 = *c23;
+            const float xx12 = mixed8s<false, false>(c12, S), xx13 = p(14), xx23 = p(19);
+            a.f4[i] = f(0) + (m(1) * d19 + m(2) * d20 + m(3) * d21 + m(6) * xx12 + m(5) * xx13 + m(4) * xx23);
+            a.f5[i] = f(1) + (m(2) * d19 + m(7) * d20 + m(8) * d21 + m(11) * xx12 + m(10) * xx13 + m(9) * xx23);
+            a.f6[i] = f(2) + (m(3) * d19 + m(8) * d20 + m(12) * d21 + m(15) * xx12 + m(14) * xx13 + m(13) * xx23);
+            const float xy11 = mixed8s<true, true>(c11, S), xy22 = mixed8s<true, true>(c22, S);
+            const float xy33 = mixed8s<true, true>(c33, S), xy13 = p(15), xy23 = p(18);
+            a.f7[i] = f(3) + (m(6) * xy11 + m(11) * xy22 + m(15) * xy33 + m(20) * xy13 + m(18) * xy23 + m(21) * d22);
+            const float xz11 = p(10), xz22 = p(16), xz33 = p(20), xz12 = p(13);
+            const float xz23 = mixed8s<true, false>(c23, S);
+            a.f8[i] = f(4) + (m(5) * xz11 + m(10) * xz22 + m(14) * xz33 + m(20) * xz12 + m(17) * xz23 + m(19) * d24);
+            const float yz11 = p(11), yz22 = p(17), yz33 = p(21), yz12 = p(12);
+            const float yz13 = mixed8s<false, true>(c13, S);
+            a.f9[i] = f(5) + (m(4) * yz11 + m(9) * yz22 + m(13) * yz33 + m(18) * yz12 + m(17) * yz13 + m(16) * d26);
+        }
+        __syncthreads();  // buffer b is refilled next iteration
+    }
 }
 
 // vPlainKernel (simulator3SetUp.cu:820-979): the velocity update.  As for
@@ -335,12 +398,13 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vplain(float* __restrict__ f1, 
     __shared__ __align__(16) float t7[2][E3Y + 8][E3X + 8];                   // x and y taps
     __shared__ __align__(16) float tm[2][E3Y + 1][E3X + 4];                   // M22: rows y0-1.., cols x0-4..
     __shared__ __align__(16) float tv[2][3][E3Y][E3X];                        // f1, f2, f3
+    __shared__ __align__(16) float tw[2][3][E3Y][E3X];  // f6, f8, f9 of plane iz+4 (the windows' new plane)
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * E3X + tx;
     const int x0 = 4 + blockIdx.x * E3X, y0 = 4 + blockIdx.y * E3Y;
     const int ix = x0 + tx, iy = y0 + ty;
     const bool act = ix < 4 + g.nx && iy < 4 + g.ny;
     const float invd1 = 1.01f, invd2 = 2.01f;
-    const int64_t sy = g.ldimx, sz = (int64_t)g.ldimx * g.ldimy;
+    const int64_t sz = (int64_t)g.ldimx * g.ldimy;
     const int z0 = 4 + blockIdx.z * E3ZC, z1 = min(z0 + E3ZC, 4 + g.nz);
     float w6[9] = {}, w8[9] = {}, w9[9] = {};  // planes iz-4 .. iz+4
     float m22z = 0.0f;
@@ -366,20 +430,22 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_vplain(float* __restrict__ f1, 
         stage_tile_async<V>(tv[b][0], f1 + pb, x0, y0, g, tid);
         stage_tile_async<V>(tv[b][1], f2 + pb, x0, y0, g, tid);
         stage_tile_async<V>(tv[b][2], f3 + pb, x0, y0, g, tid);
+        const int64_t pw = pb + 4 * sz;
+        stage_tile_async<V>(tw[b][0], f6 + pw, x0, y0, g, tid);
+        stage_tile_async<V>(tw[b][1], f8 + pw, x0, y0, g, tid);
+        stage_tile_async<V>(tw[b][2], f9 + pw, x0, y0, g, tid);
         __pipeline_commit();
     };
     if (z0 < z1) stage(0, z0);
     for (int iz = z0, b = 0; iz < z1; ++iz, b ^= 1) {
         const int64_t i = g.idx(ix, iy, iz);
         if (iz + 1 < z1) stage(b ^ 1, iz + 1);
-        if (act) {
-            zshift(w6, f6, i + 4 * sz);
-            zshift(w8, f8, i + 4 * sz);
-            zshift(w9, f9, i + 4 * sz);
-        }
         __pipeline_wait_prior(iz + 1 < z1 ? 1 : 0);
         __syncthreads();
         if (act) {
+            zpush(w6, tw[b][0][ty][tx]);
+            zpush(w8, tw[b][1][ty][tx]);
+            zpush(w9, tw[b][2][ty][tx]);
             const float m22c = tm[b][ty + 1][tx + 4], mx = tm[b][ty + 1][tx + 3], my = tm[b][ty][tx + 4];
             const float d10 = drv8s<true>(&t4[b][ty][tx + 4], 1), d11 = drv8s<true>(&t5[b][ty + 4][tx], E3X);
             const float d12 = zdrv(w6, true);
@@ -557,7 +623,19 @@ int tti_e3_launch_splain(float* f4, float* f5, float* f6, float* f7, float* f8, 
     a.e23 = f2_3;
     a.e33 = f3_3;
     for (int k = 0; k < 12; ++k) a.p[k] = p[k];
-    k_e3_splain<<<e3_blocks(g, 1), t, 0, st>>>(a, g);
+    const dim3 sb = e3_blocks(g, E3ZS);
+    if (cudaFuncSetAttribute(k_e3_splain<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)E3S_SMEM) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_e3_splain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)E3S_SMEM) !=
+            cudaSuccess)
+        return TTI_ELAUNCH;
+    if (vec4_ok(ldimx, {f4, f5, f6, f7, f8, f9, f1_1, f1_2, f1_3, f2_2, f2_3, f3_3}) &&
+        vec4_ok(ldimx, {M[0], M[1], M[2], M[3], M[4], M[5], M[6], M[7], M[8], M[9], M[10], M[11], M[12], M[13],
+                        M[14], M[15], M[16], M[17], M[18], M[19], M[20]}) &&
+        vec4_ok(ldimx, {p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8], p[9], p[10], p[11]}))
+        k_e3_splain<4><<<sb, t, E3S_SMEM, st>>>(a, g);
+    else
+        k_e3_splain<1><<<sb, t, E3S_SMEM, st>>>(a, g);
     return launch_status();
 }
 
@@ -569,7 +647,7 @@ int tti_e3_launch_vplain(float* f1, float* f2, float* f3, const float* f4, const
         !M22 || !zprime)
         return TTI_EINVAL;
     const E3Grid g{nx, ny, nz, ldimx, ldimy};
-    if (vec4_ok(ldimx, {f1, f2, f3, f4, f5, f7, f8, f9, M22}))
+    if (vec4_ok(ldimx, {f1, f2, f3, f4, f5, f6, f7, f8, f9, M22}))
         k_e3_vplain<4><<<e3_blocks(g, E3ZC), dim3(E3X, E3Y), 0, S(stream)>>>(f1, f2, f3, f4, f5, f6, f7, f8, f9, M22,
                                                                              zprime, g);
     else
