@@ -7,10 +7,12 @@
 // interpolation tables are {1.01, 2.01, 3.01, 4.01}, its inverse spacings
 // are hard-coded (1.01, 2.01 or 2.02, and zprime[iz] in z), and its model
 // is cos/sin of the cell indices.  These kernels reproduce it as it is, so
-// that its step can be dropped in; they compute one cell per thread with the
-// z planes of a column split over a few threads, and read the stencil taps
-// through the L1 cache (the reused neighbours of a 32-wide warp row stay
-// there), which suits these short, single-pass stencils.
+// that its step can be dropped in.  They are short single-pass stencils
+// over many volumes: blocks of 32x8 threads walk z through a column tile,
+// every operand of a plane staged in double-buffered shared tiles by
+// asynchronous copies while the previous plane is used, and z taps kept in
+// per-thread register windows (the reference's shared planes and register
+// queues, with the copies in flight a plane ahead).
 //
 // Volumes: FP32, x fastest, radius-4 halo on every axis, interior cells
 // [4, 4+n-1] per axis, idx = (iz*ldimy + iy)*ldimx + ix.
@@ -41,30 +43,6 @@ __device__ __forceinline__ float e3_int(int i)
     return c[i];
 }
 
-// drv1_8<SHIFT, STRIDE> (simulator3SetUp.cu:37-45)
-template <bool SHIFT>
-__device__ __forceinline__ float drv8(const float* __restrict__ p, int64_t s)
-{
-    constexpr int is = SHIFT ? -1 : 0;
-    float d = e3_df(0) * (__ldg(p + (is + 1) * s) - __ldg(p + is * s));
-#pragma unroll
-    for (int i = 1; i < 4; ++i) d += e3_df(i) * (__ldg(p + (is + i + 1) * s) - __ldg(p + (is - i) * s));
-    return d;
-}
-
-// mixed_XY<XS, YS> (simulator3SetUp.cu:214-227)
-template <bool XS, bool YS>
-__device__ __forceinline__ float mixed8(const float* __restrict__ p, int64_t sy)
-{
-    constexpr int xs = XS ? -1 : 0, ys = YS ? -1 : 0;
-    float d = 0.0f;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-        d += e3_int(i) * (__ldg(p + (ys + i + 1) * sy + xs + i + 1) + __ldg(p + (ys + i + 1) * sy + xs - i) +
-                          __ldg(p + (ys - i) * sy + xs + i + 1) + __ldg(p + (ys - i) * sy + xs - i));
-    return 0.5f * d;
-}
-
 struct E3Grid {
     int nx, ny, nz, ldimx, ldimy;
     __device__ int64_t idx(int ix, int iy, int iz) const { return ((int64_t)iz * ldimy + iy) * ldimx + ix; }
@@ -92,7 +70,8 @@ __device__ __forceinline__ void zpush(float (&w)[9], float v)
     w[8] = v;
 }
 
-// drv1_8 on a shared-memory tile (stride s between taps).
+// drv1_8<SHIFT, STRIDE> (simulator3SetUp.cu:37-45) on a shared-memory tile
+// (stride s between taps).
 template <bool SHIFT>
 __device__ __forceinline__ float drv8s(const float* p, int s)
 {
@@ -103,23 +82,12 @@ __device__ __forceinline__ float drv8s(const float* p, int s)
     return d;
 }
 
-// Stage rows ys .. ys+R-1, columns xs .. xs+C-1 of one plane into t (zero
-// past the allocation's row or plane end; no output reads those cells).
-template <int R, int C>
-__device__ __forceinline__ void stage_tile(float (&t)[R][C], const float* __restrict__ plane, int xs, int ys,
-                                           const E3Grid& g, int tid)
-{
-    for (int e = tid; e < R * C; e += E3X * E3Y) {
-        const int r = e / C, c = e - r * C, x = xs + c, y = ys + r;
-        t[r][c] = (x < g.ldimx && y < g.ldimy) ? __ldg(plane + (int64_t)y * g.ldimx + x) : 0.0f;
-    }
-}
-
-// The same, issued as asynchronous copies (LDGSTS) of V floats (1, or 4
-// when ldimx is a multiple of 4 and the volumes are 16-byte aligned: then
-// xs being a multiple of 4, a chunk lies wholly inside or wholly past a
-// row's end) into t; the caller commits and waits.  Cells past the
-// allocation's row or plane end are zeroed directly.
+// Stage rows ys .. ys+R-1, columns xs .. xs+C-1 of one plane into t by
+// asynchronous copies (LDGSTS) of V floats (1, or 4 when ldimx is a
+// multiple of 4 and the volumes are 16-byte aligned: then, xs being a
+// multiple of 4, a chunk lies wholly inside or wholly past a row's end);
+// the caller commits and waits.  Cells past the allocation's row or plane
+// end are zeroed directly (no interior output reads them).
 template <int V, int R, int C>
 __device__ __forceinline__ void stage_tile_async(float (&t)[R][C], const float* __restrict__ plane, int xs, int ys,
                                                  const E3Grid& g, int tid)
@@ -291,7 +259,8 @@ struct E3Stress {
     const float* p[12];                             // f10 .. f21
 };
 
-// mixed_XY on a shared-memory tile (row stride sy).
+// mixed_XY<XS, YS> (simulator3SetUp.cu:214-227) on a shared-memory tile
+// (row stride sy).
 template <bool XS, bool YS>
 __device__ __forceinline__ float mixed8s(const float* p, int sy)
 {
