@@ -194,8 +194,9 @@ template <int XS, int YS, int ZS, int V>
 __global__ void __launch_bounds__(E3X* E3Y) k_e3_precompute(const float* __restrict__ in, float* __restrict__ xz,
                                                            float* __restrict__ yz, E3Grid g)
 {
-    // planes staged in double-buffered shared tiles (halo 4) by async copies
-    __shared__ __align__(16) float t[2][E3Y + 8][E3X + 8];
+    // planes staged in triple-buffered shared tiles (halo 4) by async copies,
+    // two planes in flight while one is used
+    __shared__ __align__(16) float t[3][E3Y + 8][E3X + 8];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * E3X + tx;
     const int x0 = 4 + blockIdx.x * E3X, y0 = 4 + blockIdx.y * E3Y;
     const int ix = x0 + tx, iy = y0 + ty;
@@ -215,9 +216,10 @@ __global__ void __launch_bounds__(E3X* E3Y) k_e3_precompute(const float* __restr
         __pipeline_commit();
     };
     stage(0, 0);
-    for (int s = 0, bb = 0; s < ns; ++s, bb ^= 1) {
-        if (s + 1 < ns) stage(bb ^ 1, s + 1);
-        __pipeline_wait_prior(s + 1 < ns ? 1 : 0);
+    if (ns > 1) stage(1, 1);
+    for (int s = 0, bb = 0; s < ns; ++s, bb = bb == 2 ? 0 : bb + 1) {
+        if (s + 2 < ns) stage(bb == 0 ? 2 : bb - 1, s + 2);  // the buffer plane s-1 used
+        __pipeline_wait_prior(s + 2 < ns ? 2 : s + 1 < ns ? 1 : 0);
         __syncthreads();
         const float* pl = &t[bb][ty + 4][tx + 4];
         constexpr int S = E3X + 8;
